@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the PAVES GPU search path on B200.
+
+Workload (synthetic, seeded; stands in for SIFT1M): N = 1,000,000 rows x
+128 dims from the Gaussian-mixture generator, two attribute columns,
+batches of 64 queries whose predicates rotate through the six selectivity
+classes (0.1% .. 95%), filtered L2 top-10. A step is one batch through the
+device: predicate bitmaps, scan, merge.
+
+  value     queries/s with inputs resident in HBM, device time (CUDA events
+            on the library's stream) of K back-to-back steps, max over ranks
+  e2e       the same batch through the drop-in C ABI (fv_gpu_brute_batch)
+            with host buffers: predicate compile + H2D + kernels + D2H
+  roofline  the scan kernel: algorithmic bytes (rows once per batch) over
+            its average CUDA-event duration, against MEASURED_PEAKS.json
+  cpu_baseline  the reference engine's CPU BruteCursor (oracle/_ref, built
+            from the reference sources) on a bounded sample, all host cores
+
+--impl reference times that reference CPU path alone (rank 0).
+Multi-GPU (torchrun): each rank serves its own batches on its own GPU
+(independent replicas, weak scaling; the scan needs no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from paves_b200 import _lib, datagen, pred  # noqa: E402
+from paves_b200.index import GpuIndex  # noqa: E402
+
+METRIC = "filtered top-10 QPS, 1M x 128 L2"
+N_ROWS, DIM, BATCH, TOPK = 1_000_000, 128, 64, 10
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.p is None:
+            return out
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows]
+        mx = [float(r[2]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nme in enumerate(names):
+                if r[5 + i].strip().lower() == "active":
+                    reasons.add(nme)
+        out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), reasons=sorted(reasons),
+                   samples=len(rows))
+        return out
+
+
+def make_workload(n=N_ROWS, d=DIM, nq=BATCH):
+    ds = datagen.make_dataset(n, d, nq=nq)
+    kinds = list(datagen.six_predicates().items())
+    preds = [kinds[q % len(kinds)][1] for q in range(nq)]
+    return ds, preds, [kinds[q % len(kinds)][0] for q in range(nq)]
+
+
+# ---------------------------------------------------------------- reference CPU
+def reference_cpu_qps(ds, preds, budget_s=20.0, threads=None):
+    """Reference engine BruteCursor (built from the reference sources), one
+    query at a time with `threads` workers, over up to len(preds) queries
+    within budget_s. Returns (qps, queries_run, threads, kind)."""
+    from oracle import refengine
+    from paves_b200.indexfile import write_index
+    threads = threads or os.cpu_count() or 1
+    n = ds.vectors.shape[0]
+    with tempfile.TemporaryDirectory(dir="/tmp") as td:
+        path = os.path.join(td, "bench.idx")
+        l0 = np.zeros((n, 3), np.uint32)  # no graph needed for the brute path (M=1)
+        write_index(path, ds.vectors, ds.cols, 1, 1, np.zeros(n, np.uint8), l0,
+                    np.zeros(n + 1, np.uint64), np.zeros(0, np.uint32), 0, 0)
+        R = refengine.RefIndex(path)
+        handles = {}
+        done = 0
+        t0 = time.perf_counter()
+        for q, p in enumerate(preds):
+            key = id(p)
+            if key not in handles:
+                handles[key] = R.compile(p)
+            R.brute(ds.queries[q], handles[key], TOPK, threads=threads)
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        dt = time.perf_counter() - t0
+        for h in handles.values():
+            R.free_pred(h)
+        R.close()
+    return done / dt, done, threads
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ds, preds, _ = make_workload()
+    per_step = []
+    for _ in range(args.warmup):
+        reference_cpu_qps(ds, preds[:8], budget_s=5.0)
+    for _ in range(args.steps):
+        qps, nrun, threads = reference_cpu_qps(ds, preds, budget_s=10.0)
+        per_step.append(qps)
+    qps = float(np.median(per_step))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(qps, 2), "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * BATCH / qps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "1M x 128 Gaussian-mixture rows, 64-query batches, six "
+                               "predicate classes, top-10, reference CPU BruteCursor",
+                   "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK},
+        "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"up to {BATCH} queries per step, one at a time"},
+        "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- ours
+def prepared_batch(gi, queries, bp, topb, mode):
+    L = _lib.lib()
+    err = C.create_string_buffer(512)
+    q = np.ascontiguousarray(queries, np.float32)
+    b = L.pv_batch_create(gi.handle, q.shape[0], _lib.ptr(q), _lib.ptr(bp.qd),
+                          _lib.ptr(bp.nodes), len(bp.nodes), _lib.ptr(bp.children),
+                          len(bp.children), _lib.ptr(bp.invals), len(bp.invals), topb, mode,
+                          err, 512)
+    if not b:
+        raise RuntimeError(err.value.decode())
+    return b
+
+
+def batch_run(b, iters, stages=False):
+    L = _lib.lib()
+    err = C.create_string_buffer(512)
+    st = (C.c_float * 4)()
+    tot = C.c_float()
+    rc = L.pv_batch_run(b, iters, st if stages else None, C.byref(tot), err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return tot.value, list(st)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    ds, preds, kinds = make_workload()
+    gi = GpuIndex(ds.vectors, ds.cols, device=local)
+    bp = pred.concat(preds, N_ROWS)
+    b = prepared_batch(gi, ds.queries, bp, TOPK, _lib.PV_MODE_EXACT)
+    batch_run(b, args.warmup)
+
+    def barrier():
+        if dist:
+            import torch
+            t = torch.zeros(1, device=f"cuda:{local}")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    barrier()
+    clk = Clocks(local)
+    total_ms, _ = batch_run(b, args.steps)
+    clocks = clk.stop()
+    barrier()
+    if dist:
+        import torch
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = BATCH * args.steps * world / (total_ms / 1e3)
+
+    # per-kernel device times of the same steps (events between kernels)
+    _, st = batch_run(b, args.steps, stages=True)
+    scan_ms = st[1] / args.steps
+    hbm, bf16, peak_kind = load_peaks()
+    alg_bytes = N_ROWS * DIM * 4  # rows once per batch
+    achieved = alg_bytes / (scan_ms / 1e3) / 1e9
+
+    # scan GB/s at batch 1 (the HBM-bound exact scan)
+    bp1 = pred.concat([preds[5]], N_ROWS)
+    b1 = prepared_batch(gi, ds.queries[:1], bp1, TOPK, _lib.PV_MODE_EXACT)
+    batch_run(b1, 3)
+    _, st1 = batch_run(b1, 20, stages=True)
+    scan1_ms = st1[1] / 20
+    scan_gbs_b1 = alg_bytes / (scan1_ms / 1e3) / 1e9
+    _lib.lib().pv_batch_free(b1)
+
+    # end to end through the drop-in ABI, host buffers
+    q = np.ascontiguousarray(ds.queries, np.float32)
+    for _ in range(3):
+        gi.brute_batch_raw(q, bp, TOPK)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        gi.brute_batch_raw(q, bp, TOPK)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_qps = BATCH * args.steps * world / e2e_s
+    h2d = q.nbytes + bp.qd.nbytes + bp.nodes.nbytes + bp.children.nbytes + bp.invals.nbytes
+    d2h = BATCH * TOPK * 16 + BATCH * 4 + BATCH
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import refengine
+            if refengine.available("cpu"):
+                qps, nrun, threads = reference_cpu_qps(ds, preds, budget_s=15.0)
+                cpu = {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
+                       "kind": "reference",
+                       "sample": f"{nrun} queries of the batch, one at a time (BruteCursor)"}
+        except Exception as e:  # baseline is informative only
+            cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"failed: {e}"}
+
+    _lib.lib().pv_batch_free(b)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "1M x 128 Gaussian-mixture rows (integer-valued), 64-query "
+                                   "batches over six predicate classes 0.1%-95%, exact FP32 "
+                                   "filtered top-10",
+                       "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK, "path": "exact",
+                       "l2_flush": "inputs larger than L2 (512 MB rows vs 126 MB)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                         "kernel": "scan_f32_kernel", "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
+            "scan_gbs_batch1": round(scan_gbs_b1, 1),
+            "stage_ms": {"bitmap": round(st[0] / args.steps, 4), "scan": round(scan_ms, 4),
+                         "merge": round(st[3] / args.steps, 4)},
+            "clocks": clocks,
+            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * args.steps,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    gi.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

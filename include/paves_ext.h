@@ -1,0 +1,67 @@
+/*
+ * paves_ext.h — additions to the drop-in ABI (libpaves_gpu.so).
+ *
+ * None of these replace a reference entry point; they sit beside the
+ * gpu_engine.h surface declared in paves_gpu.h:
+ *   - host-side predicate validation (no device needed),
+ *   - prepared batches whose inputs stay resident in device memory, for
+ *     callers that issue the same batch repeatedly or that measure the
+ *     device-side cost alone,
+ *   - per-stage device timings of the last call.
+ * Same conventions as paves_gpu.h: plain C, host pointers and sizes, 0 or
+ * -1 + errbuf.
+ */
+#ifndef PAVES_B200_EXT_H
+#define PAVES_B200_EXT_H
+
+#include "paves_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scan modes of a prepared batch. */
+#define PV_MODE_EXACT 0 /* exact FP32 scan */
+#define PV_MODE_LOW 1   /* reduced-precision (index precision) scan + FP32 re-rank */
+
+/* Validates and compiles the predicates of a batch on the host exactly as
+ * fv_gpu_brute_batch does, without touching a device. *nprog receives the
+ * number of distinct predicates. Returns 0 or -1 + errbuf. */
+int pv_pred_check(int nq, const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
+                  const int32_t *children, int nchildren, const double *invals, int ninvals,
+                  int ncols, int *nprog, char *errbuf, size_t errlen);
+
+typedef struct PvBatch PvBatch;
+
+/* Compiles the batch's predicates and copies queries + predicate programs
+ * to the device once. topb as in fv_gpu_brute_batch (nq may exceed
+ * FV_GPU_MAX_BATCH, up to 65536). */
+PvBatch *pv_batch_create(FvGpuIndex *g, int nq, const float *queries,
+                         const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
+                         const int32_t *children, int nchildren, const double *invals,
+                         int ninvals, uint32_t topb, int mode, char *errbuf, size_t errlen);
+
+/* Runs the device-side work of the batch (bitmaps, scan, re-rank, merge)
+ * iters times back to back on the index's stream and waits. stage_ms, if
+ * not NULL, receives the summed device time of each stage over the iters
+ * (4 floats: bitmap, scan, rerank, merge); *total_ms the whole. */
+int pv_batch_run(PvBatch *b, int iters, float *stage_ms, float *total_ms, char *errbuf,
+                 size_t errlen);
+
+/* Copies the last run's results to the caller (layout of fv_gpu_brute_batch). */
+int pv_batch_fetch(PvBatch *b, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
+                   char *errbuf, size_t errlen);
+
+void pv_batch_free(PvBatch *b);
+
+/* Device time (ms) of the kernels of the last synchronous batch call on g. */
+float pv_last_kernel_ms(const FvGpuIndex *g);
+
+/* Counters of the last fv_gpu_graph_batch call: per query [steps, visited,
+ * predicate probes, results]; copies min(nq, last nq) rows, returns rows. */
+int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAVES_B200_EXT_H */

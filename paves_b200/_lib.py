@@ -1,0 +1,126 @@
+"""ctypes binding of libpaves_gpu.so (the C ABI declared in include/*.h).
+
+The library is built in-tree (``paves_b200/libpaves_gpu.so``). There is no
+fallback: if the library is missing, importing a GPU entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpaves_gpu.so")
+
+FV_CMP_LT, FV_CMP_LE, FV_CMP_EQ, FV_CMP_GE, FV_CMP_GT, FV_CMP_NE = range(6)
+FV_NODE_CMP, FV_NODE_IN, FV_NODE_AND, FV_NODE_OR, FV_NODE_NOT = range(5)
+FV_GPU_PREC_FP32, FV_GPU_PREC_SQ8, FV_GPU_PREC_BF16, FV_GPU_PREC_FP8 = range(4)
+FV_GPU_MAX_TOPB = 4096
+FV_GPU_MAX_SPANS = 4096
+FV_GPU_MAX_EF = 512
+FV_GPU_MAX_BATCH = 1024
+
+
+class FvGpuPredNode(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("col", C.c_int32), ("op", C.c_int32),
+                ("nchildren", C.c_int32), ("child0", C.c_int32),
+                ("nvalues", C.c_int32), ("val0", C.c_int32), ("pad", C.c_int32),
+                ("value", C.c_double)]
+
+
+class FvGpuSpan(C.Structure):
+    _fields_ = [("col", C.c_int32), ("lo", C.c_uint32), ("hi", C.c_uint32)]
+
+
+class FvHit(C.Structure):
+    _fields_ = [("node", C.c_uint64), ("dist", C.c_float)]
+
+
+class FvGpuQueryDesc(C.Structure):
+    _fields_ = [("proot", C.c_int32), ("need_eval", C.c_int32), ("span0", C.c_int32),
+                ("nspans", C.c_int32), ("soff0", C.c_int32), ("entry", C.c_uint32),
+                ("total", C.c_uint64)]
+
+
+assert C.sizeof(FvGpuPredNode) == 40 and C.sizeof(FvGpuSpan) == 12
+assert C.sizeof(FvHit) == 16 and C.sizeof(FvGpuQueryDesc) == 32
+
+# numpy mirrors (same byte layout) for bulk construction
+NODE_DTYPE = np.dtype([("kind", "<i4"), ("col", "<i4"), ("op", "<i4"), ("nchildren", "<i4"),
+                       ("child0", "<i4"), ("nvalues", "<i4"), ("val0", "<i4"), ("pad", "<i4"),
+                       ("value", "<f8")])
+SPAN_DTYPE = np.dtype([("col", "<i4"), ("lo", "<u4"), ("hi", "<u4")])
+HIT_DTYPE = np.dtype({"names": ["node", "dist"], "formats": ["<u8", "<f4"],
+                      "offsets": [0, 8], "itemsize": 16})
+QD_DTYPE = np.dtype([("proot", "<i4"), ("need_eval", "<i4"), ("span0", "<i4"),
+                     ("nspans", "<i4"), ("soff0", "<i4"), ("entry", "<u4"), ("total", "<u8")])
+assert NODE_DTYPE.itemsize == 40 and QD_DTYPE.itemsize == 32 and SPAN_DTYPE.itemsize == 12
+
+_lib = None
+
+P = C.c_void_p
+_SIGS = {
+    "fv_gpu_available": (C.c_int, []),
+    "fv_gpu_index_upload": (P, [P, P, P, P, C.c_uint32, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                C.c_int, C.c_char_p, C.c_size_t]),
+    "fv_gpu_index_free": (None, [P]),
+    "fv_gpu_index_device": (C.c_int, [P]),
+    "fv_gpu_index_precision": (C.c_int, [P]),
+    "fv_gpu_brute_batch": (C.c_int, [P, C.c_int, P, P, P, P, C.c_int, P, C.c_int, P, C.c_int,
+                                     P, C.c_int, P, C.c_int, C.c_uint32, P, P, P, C.c_char_p,
+                                     C.c_size_t]),
+    "fv_gpu_graph_batch": (C.c_int, [P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int,
+                                     C.c_uint32, C.c_uint64, P, P, P, C.c_char_p, C.c_size_t]),
+    "fv_gpu_tile_variant_qt": (C.c_int, [C.c_int]),
+    "fv_gpu_mem_probe": (C.c_int, [P, P]),
+}
+
+
+def exported_symbols():
+    """Names the library must export: every function declared in include/*.h."""
+    return list(_SIGS) + list(_EXT_SIGS)
+
+
+_EXT_SIGS = {
+    "pv_pred_check": (C.c_int, [C.c_int, P, P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, P,
+                                C.c_char_p, C.c_size_t]),
+    "pv_batch_create": (P, [P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int, C.c_uint32,
+                            C.c_int, C.c_char_p, C.c_size_t]),
+    "pv_batch_run": (C.c_int, [P, C.c_int, P, P, C.c_char_p, C.c_size_t]),
+    "pv_batch_fetch": (C.c_int, [P, P, P, P, C.c_char_p, C.c_size_t]),
+    "pv_batch_free": (None, [P]),
+    "pv_last_kernel_ms": (C.c_float, [P]),
+    "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
+}
+PV_MODE_EXACT, PV_MODE_LOW = 0, 1
+
+
+def register_ext(name, restype, argtypes):
+    _EXT_SIGS[name] = (restype, argtypes)
+    if _lib is not None:
+        f = getattr(_lib, name)
+        f.restype, f.argtypes = restype, argtypes
+
+
+def lib():
+    """Loads libpaves_gpu.so once; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; "
+                "g.build()'` (or make -C paves_b200/csrc)")
+        L = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
+        for name, (rt, at) in list(_SIGS.items()) + list(_EXT_SIGS.items()):
+            f = getattr(L, name)
+            f.restype, f.argtypes = rt, at
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    """Address of a contiguous numpy array (None for None / empty)."""
+    if a is None:
+        return None
+    return a.ctypes.data if a.size else None

@@ -1,0 +1,210 @@
+// brute.cu — batched filtered top-K: staging, launch sequence, results.
+//
+// Replaces fv_gpu_brute_batch and its host paths (gpu_engine.cu:1776-2336).
+// One call: compile the batch's predicates on the host (pred.cpp), pack
+// queries + predicate programs into one pinned buffer and copy it with a
+// single H2D transfer, then on the index's stream
+//   bitmap_kernel  -> one packed bitmap per distinct predicate
+//   scan           -> per-CTA top-K lists + grid-wide bounds
+//   merge_kernel   -> FvHit [nq][topb], counts, truncation flags
+// and one D2H transfer of the packed results. Spans, need_eval and dedup
+// are accepted for ABI compatibility; the scan evaluates the full
+// predicate through the bitmap, which selects exactly the rows the driver
+// spans would (a covering driver equals its predicate's match set,
+// engine.cpp:464-599) and cannot produce duplicates.
+#include <string.h>
+
+#include <algorithm>
+
+#include "index.h"
+#include "pv_internal.h"
+
+namespace pv {
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                  DevBatch &db, size_t extra_bytes, char *errbuf, size_t errlen) {
+    const size_t qbytes = (size_t)nq * g->dpad * 4;
+    const int P = (int)pb.progs.size();
+    db.nq = nq;
+    db.P = P;
+    db.off_q = 0;
+    db.off_qprog = al256(qbytes);
+    db.off_progs = db.off_qprog + al256((size_t)nq * 4);
+    db.off_insns = db.off_progs + al256((size_t)P * sizeof(PredProg) + 8);
+    db.off_consts = db.off_insns + al256(pb.insns.size() * sizeof(PredInsn) + 8);
+    db.off_extra = db.off_consts + al256(pb.consts.size() * 8 + 8);
+    db.bytes = db.off_extra + al256(extra_bytes);
+    PV_CUDA_OK(db.stage_h->ensure(db.bytes), errbuf, errlen);
+    PV_CUDA_OK(db.stage_d->ensure(db.bytes), errbuf, errlen);
+    char *h = db.stage_h->as<char>();
+    float *hq = (float *)(h + db.off_q);
+    if (g->dpad == g->dim) {
+        memcpy(hq, queries, qbytes);
+    } else {
+        for (int q = 0; q < nq; q++) {
+            memcpy(hq + (size_t)q * g->dpad, queries + (size_t)q * g->dim, (size_t)g->dim * 4);
+            memset(hq + (size_t)q * g->dpad + g->dim, 0, (size_t)(g->dpad - g->dim) * 4);
+        }
+    }
+    memcpy(h + db.off_qprog, pb.qprog.data(), (size_t)nq * 4);
+    if (P) memcpy(h + db.off_progs, pb.progs.data(), (size_t)P * sizeof(PredProg));
+    if (!pb.insns.empty())
+        memcpy(h + db.off_insns, pb.insns.data(), pb.insns.size() * sizeof(PredInsn));
+    if (!pb.consts.empty()) memcpy(h + db.off_consts, pb.consts.data(), pb.consts.size() * 8);
+    return 0;
+}
+
+int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen) {
+    PV_CUDA_OK(cudaMemcpyAsync(db.stage_d->p, db.stage_h->p, db.bytes, cudaMemcpyHostToDevice,
+                               g->stream),
+               errbuf, errlen);
+    return 0;
+}
+
+// Device-side work of one batch: inputs already resident in db.stage_d.
+int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
+                 uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
+                 cudaEvent_t *ev) {
+    const int nq = db.nq, P = db.P;
+    char *d = db.stage_d->as<char>();
+    const float *d_q = (const float *)(d + db.off_q);
+    const int32_t *d_qprog = (const int32_t *)(d + db.off_qprog);
+    const PredProg *d_progs = (const PredProg *)(d + db.off_progs);
+    const PredInsn *d_insns = (const PredInsn *)(d + db.off_insns);
+    const double *d_consts = (const double *)(d + db.off_consts);
+    const uint64_t bm_words = (g->count + 31) / 32;
+    ScanScratch &s = g->scan;
+
+    if (ev) cudaEventRecord(ev[0], g->stream);
+    if (P > 0) {
+        PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
+        PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
+        PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,
+                                  s.bitmaps.as<uint32_t>(), bm_words,
+                                  s.popcnt.as<unsigned long long>(), g->sm_count, g->stream),
+                   errbuf, errlen);
+    } else {
+        PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
+    }
+    (void)mode;
+
+    ScanPlan pl;
+    if (!plan_scan_f32(g->count, g->dpad, nq, (int)topb, g->sm_count, pl)) {
+        snprintf(errbuf, errlen, "gpu: dimension %d not supported by the scan", g->dim);
+        return -1;
+    }
+    PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
+    PV_CUDA_OK(s.part.ensure((size_t)nq * pl.grow * topb * 8), errbuf, errlen);
+    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * pl.grow * 4), errbuf, errlen);
+    PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
+
+    ScanF32Args a;
+    a.vecs = g->d_vecs;
+    a.nrows = g->count;
+    a.dpad = g->dpad;
+    a.queries = d_q;
+    a.nq = nq;
+    a.bitmaps = s.bitmaps.as<uint32_t>();
+    a.bm_words = bm_words;
+    a.qprog = d_qprog;
+    a.K = (int)topb;
+    a.S = pl.S;
+    a.CB = pl.CB;
+    a.rows_per_cta = pl.rows_per_cta;
+    a.grow = pl.grow;
+    a.qtiles = pl.qtiles;
+    a.tau = s.tau.as<unsigned long long>();
+    a.part = s.part.as<uint64_t>();
+    a.part_cnt = s.part_cnt.as<uint32_t>();
+    if (ev) cudaEventRecord(ev[1], g->stream);
+    PV_CUDA_OK(launch_scan_f32(a, pl, g->stream), errbuf, errlen);
+    if (ev) {
+        cudaEventRecord(ev[2], g->stream);
+        cudaEventRecord(ev[3], g->stream);
+    }
+    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, pl.grow, (int)topb, pl, a.tau, d_qprog,
+                            s.popcnt.as<unsigned long long>(), g->count, nq, d_out, d_cnt,
+                            d_trunc, g->stream),
+               errbuf, errlen);
+    if (ev) cudaEventRecord(ev[4], g->stream);
+    return 0;
+}
+
+}  // namespace pv
+
+using namespace pv;
+
+extern "C" int fv_gpu_tile_variant_qt(int dim) {
+    if (dim <= 0) return 0;
+    return scan_f32_max_qt(dim);
+}
+
+extern "C" int fv_gpu_brute_batch(FvGpuIndex *g, int nq, const float *queries,
+                                  const FvGpuQueryDesc *qd, const uint8_t *dedup,
+                                  const FvGpuPredNode *nodes, int nnodes,
+                                  const int32_t *children, int nchildren,
+                                  const double *invals, int ninvals, const FvGpuSpan *spans,
+                                  int nspans_total, const uint64_t *spanoff, int nspanoff,
+                                  uint32_t topb, FvHit *out, uint32_t *out_cnt,
+                                  uint8_t *truncated, char *errbuf, size_t errlen) {
+    (void)dedup;
+    (void)spans;
+    (void)spanoff;
+    (void)nspanoff;
+    if (!g || nq < 1 || nq > FV_GPU_MAX_BATCH || topb == 0 || topb > FV_GPU_MAX_TOPB ||
+        nspans_total > FV_GPU_MAX_SPANS * nq || !queries || !qd || !out || !out_cnt ||
+        !truncated) {
+        if (errbuf && errlen)
+            snprintf(errbuf, errlen, "gpu: bad brute batch (nq=%d topb=%u)", nq, topb);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(g->mu);
+    PV_CUDA_OK(cudaSetDevice(g->device), errbuf, errlen);
+    PredBatch pb;
+    if (compile_predicates(nq, &qd[0].proot, sizeof(FvGpuQueryDesc), nodes, nnodes, children,
+                           nchildren, invals, ninvals, g->ncols, pb, errbuf, errlen) != 0)
+        return -1;
+    return brute_run_host(g, nq, queries, pb, topb, FV_GPU_PREC_FP32 == g->precision ? 0 : 1,
+                          out, out_cnt, truncated, errbuf, errlen);
+}
+
+namespace pv {
+
+int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                   uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
+                   char *errbuf, size_t errlen) {
+    DevBatch db;
+    db.stage_h = &g->scan.stage_h;
+    db.stage_d = &g->scan.stage_d;
+    if (brute_prepare(g, nq, queries, pb, db, 0, errbuf, errlen)) return -1;
+    const size_t hit_bytes = (size_t)nq * topb * sizeof(FvHit);
+    const size_t off_cnt = al256(hit_bytes);
+    const size_t off_tr = off_cnt + al256((size_t)nq * 4);
+    const size_t obytes = off_tr + al256((size_t)nq);
+    PV_CUDA_OK(g->scan.out_d.ensure(obytes), errbuf, errlen);
+    PV_CUDA_OK(g->scan.out_h.ensure(obytes), errbuf, errlen);
+    char *od = g->scan.out_d.as<char>();
+    if (brute_upload(g, db, errbuf, errlen)) return -1;
+    cudaEventRecord(g->ev0, g->stream);
+    if (brute_launch(g, db, topb, mode, (FvHit *)od, (uint32_t *)(od + off_cnt),
+                     (uint8_t *)(od + off_tr), errbuf, errlen, nullptr))
+        return -1;
+    cudaEventRecord(g->ev1, g->stream);
+    PV_CUDA_OK(cudaMemcpyAsync(g->scan.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream),
+               errbuf, errlen);
+    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    cudaEventElapsedTime(&g->last_kernel_ms, g->ev0, g->ev1);
+    const char *oh = g->scan.out_h.as<char>();
+    const uint32_t *cnt = (const uint32_t *)(oh + off_cnt);
+    for (int q = 0; q < nq; q++) {
+        uint32_t c = cnt[q] > topb ? topb : cnt[q];
+        memcpy(out + (size_t)q * topb, oh + (size_t)q * topb * sizeof(FvHit), c * sizeof(FvHit));
+        out_cnt[q] = c;
+    }
+    memcpy(truncated, oh + off_tr, (size_t)nq);
+    return 0;
+}
+
+}  // namespace pv

@@ -1,0 +1,306 @@
+// index.cu — device-resident index: upload, layout conversion, release.
+//
+// Replaces fv_gpu_index_upload / fv_gpu_index_free / pick_device
+// (gpu_engine.cu:1518-1773). The resident layout differs from the
+// reference's on purpose:
+//  * exact rows stay FP32 with the row stride rounded to 16 bytes, so a
+//    warp fetches a 128-dim row in one 16-byte-per-lane load;
+//  * reduced precision (BF16 / FP8-E4M3 with a per-row scale) is an extra
+//    copy beside the FP32 rows, which the exact re-rank reads; the row
+//    stride is padded to a multiple of 64 elements (128 B for BF16) for the
+//    tensor-core scan; per-row squared norms of the stored representation
+//    feed the norm-form distance;
+//  * the level-0 graph ([cnt, neigh...] rows of stride 2M+1) becomes a
+//    fixed-width adjacency of deg_cap = 2M u32 slots padded with
+//    UINT32_MAX plus a u16 degree array: 128-byte aligned neighbour rows;
+//  * attribute columns stay f64 (predicate semantics are f64 compares).
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "index.h"
+
+namespace pv {
+
+// fp32 rows -> bf16 rows (zero padded to kpad) + squared norm of the bf16 row
+__global__ void to_bf16_kernel(const float *__restrict__ src, int dpad, int dim,
+                               uint64_t nrows, __nv_bfloat16 *__restrict__ dst, int kpad,
+                               float *__restrict__ norm) {
+    const int lane = threadIdx.x & 31;
+    uint64_t row = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (row >= nrows) return;
+    float acc = 0.f;
+    for (int j = lane; j < kpad; j += 32) {
+        float v = j < dim ? src[row * dpad + j] : 0.f;
+        __nv_bfloat16 b = __float2bfloat16_rn(v);
+        dst[row * kpad + j] = b;
+        float r = __bfloat162float(b);
+        acc = fmaf(r, r, acc);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) norm[row] = acc;
+}
+
+// fp32 rows -> fp8-e4m3 rows with one scale per row (absmax / 448), plus
+// the squared norm of the dequantized row.
+__global__ void to_fp8_kernel(const float *__restrict__ src, int dpad, int dim,
+                              uint64_t nrows, __nv_fp8_e4m3 *__restrict__ dst, int kpad,
+                              float *__restrict__ scale, float *__restrict__ norm) {
+    const int lane = threadIdx.x & 31;
+    uint64_t row = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (row >= nrows) return;
+    float amax = 0.f;
+    for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(src[row * dpad + j]));
+    for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const float s = amax > 0.f ? amax / 448.f : 1.f;
+    const float inv = 1.f / s;
+    float acc = 0.f;
+    for (int j = lane; j < kpad; j += 32) {
+        float v = j < dim ? src[row * dpad + j] * inv : 0.f;
+        __nv_fp8_e4m3 b(v);
+        dst[row * kpad + j] = b;
+        float r = float(b) * s;
+        acc = fmaf(r, r, acc);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        norm[row] = acc;
+        scale[row] = s;
+    }
+}
+
+// [cnt, n0, n1, ...] rows of stride l0_stride -> fixed-width adjacency.
+// Out-of-range neighbour ids are dropped (they would otherwise be followed).
+__global__ void adj_kernel(const uint32_t *__restrict__ l0, uint32_t l0_stride,
+                           uint64_t nrows, int deg_cap, uint32_t *__restrict__ adj,
+                           uint16_t *__restrict__ deg) {
+    uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= nrows) return;
+    const uint32_t *src = l0 + row * l0_stride;
+    uint32_t cnt = src[0];
+    if (cnt > l0_stride - 1) cnt = l0_stride - 1;
+    int n = 0;
+    for (uint32_t i = 0; i < cnt && n < deg_cap; i++) {
+        uint32_t v = src[1 + i];
+        if (v < nrows) adj[row * deg_cap + n++] = v;
+    }
+    deg[row] = (uint16_t)n;
+    for (int i = n; i < deg_cap; i++) adj[row * deg_cap + i] = 0xFFFFFFFFu;
+}
+
+static int pick_device(size_t need) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        (void)cudaGetLastError();
+        return -1;
+    }
+    int best = -1;
+    size_t bestfree = 0;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int i = 0; i < n; i++) {
+        if (cudaSetDevice(i) != cudaSuccess) continue;
+        size_t f = 0, t = 0;
+        if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        if (f > bestfree && f > need + (512ull << 20)) {
+            bestfree = f;
+            best = i;
+        }
+    }
+    cudaSetDevice(best >= 0 ? best : cur);
+    (void)cudaGetLastError();
+    return best;
+}
+
+static bool rows_integral_exact(const float *v, uint64_t count, int dim) {
+    // the norm form ||x||^2 + ||q||^2 - 2 x.q is exact in fp32 for integer
+    // rows when every partial sum stays below 2^24 (bf16 holds integers up
+    // to 256 exactly)
+    float amax = 0.f;
+    for (uint64_t i = 0; i < count * (uint64_t)dim; i++) {
+        float x = v[i];
+        if (x != floorf(x)) return false;
+        float a = fabsf(x);
+        if (a > amax) amax = a;
+        if (amax > 256.f) return false;
+    }
+    double worst = 4.0 * (double)dim * amax * amax;  // ||x||^2+||q||^2+2|x.q|
+    return worst < 16777216.0;
+}
+
+}  // namespace pv
+
+using namespace pv;
+
+extern "C" int fv_gpu_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return n > 0;
+}
+
+extern "C" int fv_gpu_index_device(const FvGpuIndex *g) { return g ? g->device : -1; }
+extern "C" int fv_gpu_index_precision(const FvGpuIndex *g) { return g ? g->precision : -1; }
+
+extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
+    if (!g) return;
+    if (g->device >= 0) cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    cudaFree(g->d_vecs);
+    cudaFree(g->d_cols);
+    cudaFree(g->d_prows);
+    cudaFree(g->d_adj);
+    cudaFree(g->d_deg);
+    cudaFree(g->d_vlow);
+    cudaFree(g->d_vscale);
+    cudaFree(g->d_norm);
+    Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
+                   &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
+                   &g->scan.out_d, &g->scan.out_h, &g->graph.visited, &g->graph.res,
+                   &g->graph.stats};
+    for (Buf *b : bufs) b->release();
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *cols,
+                                           const uint32_t *post_rows, const uint32_t *l0,
+                                           uint32_t l0_stride, uint64_t count, int dim,
+                                           int ncols, int device, int precision,
+                                           char *errbuf, size_t errlen) {
+    auto fail = [&](const char *what, cudaError_t e) -> FvGpuIndex * {
+        if (errbuf && errlen)
+            snprintf(errbuf, errlen, "gpu: index upload: %s%s%s", what, e ? ": " : "",
+                     e ? cudaGetErrorString(e) : "");
+        return nullptr;
+    };
+    if (!vectors || count == 0 || dim <= 0) return fail("empty index", cudaSuccess);
+    if (count >= 0xFFFFFFFFull) return fail("too many rows (row ids are u32)", cudaSuccess);
+    if (ncols < 0 || ncols > 32) return fail("ncols out of range", cudaSuccess);
+    if (ncols > 0 && (!cols || !post_rows)) return fail("columns missing", cudaSuccess);
+    if (precision < FV_GPU_PREC_FP32 || precision > FV_GPU_PREC_FP8)
+        return fail("unknown precision", cudaSuccess);
+    if (l0 && l0_stride < 2) return fail("bad l0 stride", cudaSuccess);
+
+    const int dpad = (dim + 3) & ~3;
+    const int kpad = (dim + 63) & ~63;
+    size_t need = count * (size_t)dpad * 4 + count * (size_t)ncols * 12;
+    if (l0) need += count * (size_t)(l0_stride - 1) * 4 + count * 2;
+    if (precision != FV_GPU_PREC_FP32) need += count * (size_t)kpad * 2 + count * 8;
+    if (device < 0) device = pick_device(need);
+    if (device < 0) return fail("no CUDA device with enough free memory", cudaSuccess);
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail("cudaSetDevice", e);
+
+    FvGpuIndex *g = new FvGpuIndex();
+    g->device = device;
+    g->precision = precision;
+    g->count = count;
+    g->dim = dim;
+    g->ncols = ncols;
+    g->l0_stride = l0 ? l0_stride : 0;
+    g->dpad = dpad;
+    g->kpad = kpad;
+    cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, device);
+    auto bail = [&](const char *what, cudaError_t err) -> FvGpuIndex * {
+        fail(what, err);
+        fv_gpu_index_free(g);
+        return nullptr;
+    };
+    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail("stream", e);
+    cudaEventCreate(&g->ev0);
+    cudaEventCreate(&g->ev1);
+
+    if ((e = cudaMalloc(&g->d_vecs, count * (size_t)dpad * 4)) != cudaSuccess)
+        return bail("rows", e);
+    if (dpad == dim) {
+        e = cudaMemcpy(g->d_vecs, vectors, count * (size_t)dim * 4, cudaMemcpyHostToDevice);
+    } else {
+        if ((e = cudaMemset(g->d_vecs, 0, count * (size_t)dpad * 4)) == cudaSuccess)
+            e = cudaMemcpy2D(g->d_vecs, (size_t)dpad * 4, vectors, (size_t)dim * 4,
+                             (size_t)dim * 4, count, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) return bail("rows copy", e);
+
+    if (ncols > 0) {
+        if ((e = cudaMalloc(&g->d_cols, count * (size_t)ncols * 8)) != cudaSuccess)
+            return bail("columns", e);
+        if ((e = cudaMemcpy(g->d_cols, cols, count * (size_t)ncols * 8,
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("columns copy", e);
+        if ((e = cudaMalloc(&g->d_prows, count * (size_t)ncols * 4)) != cudaSuccess)
+            return bail("postings", e);
+        if ((e = cudaMemcpy(g->d_prows, post_rows, count * (size_t)ncols * 4,
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("postings copy", e);
+    }
+
+    if (l0) {
+        g->deg_cap = (int)l0_stride - 1;
+        uint32_t *d_l0 = nullptr;
+        if ((e = cudaMalloc(&d_l0, count * (size_t)l0_stride * 4)) != cudaSuccess)
+            return bail("graph staging", e);
+        e = cudaMemcpy(d_l0, l0, count * (size_t)l0_stride * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&g->d_adj, count * (size_t)g->deg_cap * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&g->d_deg, count * 2);
+        if (e == cudaSuccess) {
+            adj_kernel<<<(unsigned)((count + 255) / 256), 256, 0, g->stream>>>(
+                d_l0, l0_stride, count, g->deg_cap, g->d_adj, g->d_deg);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+        cudaFree(d_l0);
+        if (e != cudaSuccess) return bail("graph", e);
+    }
+
+    g->int_exact = rows_integral_exact(vectors, count, dim);
+
+    if (precision != FV_GPU_PREC_FP32) {
+        const bool f8 = precision == FV_GPU_PREC_FP8;
+        const size_t esz = f8 ? 1 : 2;
+        if ((e = cudaMalloc(&g->d_vlow, count * (size_t)kpad * esz)) != cudaSuccess)
+            return bail("low-precision rows", e);
+        if ((e = cudaMalloc(&g->d_norm, count * 4)) != cudaSuccess) return bail("norms", e);
+        unsigned blocks = (unsigned)((count + 7) / 8);
+        if (f8) {
+            if ((e = cudaMalloc(&g->d_vscale, count * 4)) != cudaSuccess)
+                return bail("scales", e);
+            to_fp8_kernel<<<blocks, 256, 0, g->stream>>>(g->d_vecs, dpad, dim, count,
+                                                         (__nv_fp8_e4m3 *)g->d_vlow, kpad,
+                                                         g->d_vscale, g->d_norm);
+        } else {
+            to_bf16_kernel<<<blocks, 256, 0, g->stream>>>(g->d_vecs, dpad, dim, count,
+                                                          (__nv_bfloat16 *)g->d_vlow, kpad,
+                                                          g->d_norm);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return bail("convert", e);
+        if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail("convert", e);
+    }
+    return g;
+}
+
+extern "C" int fv_gpu_mem_probe(uint64_t *free_bytes, uint64_t *total_bytes) {
+    static int probed = -2;
+    if (probed == -2) probed = pick_device(0);
+    if (probed < 0) return -1;
+    size_t f = 0, t = 0;
+    if (cudaSetDevice(probed) != cudaSuccess || cudaMemGetInfo(&f, &t) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1;
+    }
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return probed;
+}

@@ -1,0 +1,108 @@
+// index.h — device-resident index layout and per-call staging (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace pv {
+
+// Grow-only device or pinned-host buffer. A buffer keeps its kind for life
+// (device memory is never released with the pinned-host call or the reverse).
+struct Buf {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool host = false;
+    explicit Buf(bool pinned_host = false) : host(pinned_host) {}
+    cudaError_t ensure(size_t need) {
+        if (need <= cap) return cudaSuccess;
+        release();
+        size_t n = need + need / 4 + 256;
+        cudaError_t e = host ? cudaMallocHost(&p, n) : cudaMalloc(&p, n);
+        if (e == cudaSuccess) cap = n;
+        else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) {
+            if (host) cudaFreeHost(p); else cudaFree(p);
+        }
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T> T *as() const { return (T *)p; }
+};
+
+// Host-compiled predicates of one batch (see pred.cpp).
+struct PredBatch {
+    std::vector<PredInsn> insns;
+    std::vector<PredProg> progs;
+    std::vector<double> consts;
+    std::vector<int32_t> qprog;  // per query: program id or -1
+    std::vector<int32_t> cols_used;  // per program: bit mask of columns (<=32)
+};
+
+// Per-call scratch for the scan path (device unless noted).
+struct ScanScratch {
+    Buf stage_h{true};   // pinned: packed inputs
+    Buf stage_d;         // device copy of the packed inputs
+    Buf bitmaps;         // [P][bm_words] u32
+    Buf popcnt;          // [P] u64
+    Buf tau;             // [nq] u64
+    Buf part;            // [nq][grow][K] u64 keys
+    Buf part_cnt;        // [nq][grow] u32
+    Buf cand;            // reduced-precision candidate superset keys
+    Buf out_d;           // FvHit [nq][topb] + cnt [nq] + trunc [nq]
+    Buf out_h{true};
+};
+
+struct GraphScratch {
+    Buf visited;  // per query overflow bitmap (words), zeroed by the kernel
+    Buf res;      // per query results
+    Buf stats;    // per query counters
+};
+
+}  // namespace pv
+
+// The opaque handle of the C ABI.
+struct FvGpuIndex {
+    int device = -1;
+    int precision = FV_GPU_PREC_FP32;
+    uint64_t count = 0;
+    int dim = 0;
+    int ncols = 0;
+    uint32_t l0_stride = 0;
+
+    int dpad = 0;            // f32 row stride in floats (dim rounded up to 4)
+    float *d_vecs = nullptr; // [count][dpad] exact rows (always resident)
+    double *d_cols = nullptr;     // [ncols][count]
+    uint32_t *d_prows = nullptr;  // [ncols][count]
+
+    // level-0 graph as fixed-degree device adjacency ("device CSR"):
+    // d_adj[node*deg_cap + i], padded with UINT32_MAX; d_deg[node]
+    uint32_t *d_adj = nullptr;
+    uint16_t *d_deg = nullptr;
+    int deg_cap = 0;
+
+    // reduced-precision copies (precision != FP32)
+    int kpad = 0;               // bf16/fp8 row stride in elements
+    void *d_vlow = nullptr;     // bf16 [count][kpad] or fp8 [count][kpad]
+    float *d_vscale = nullptr;  // fp8 per-row scale
+    float *d_norm = nullptr;    // ||x||^2 of the stored low-precision row
+    bool int_exact = false;     // rows integral, |x| <= 256, d*max^2 < 2^24
+
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;  // ABI calls are serialized per handle
+
+    pv::ScanScratch scan;
+    pv::GraphScratch graph;
+    float last_kernel_ms = 0.f;  // device time of the last batch's kernels
+    std::vector<uint32_t> graph_stats;  // last graph batch: [nq][4] counters
+};

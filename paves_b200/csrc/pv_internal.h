@@ -1,0 +1,80 @@
+// pv_internal.h — declarations shared between the library's sources.
+#pragma once
+
+#include "index.h"
+
+namespace pv {
+
+// ---- predicates (pred.cpp, bitmap.cu)
+int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
+                       const FvGpuPredNode *nodes, int nnodes, const int32_t *children,
+                       int nchildren, const double *invals, int ninvals, int ncols,
+                       PredBatch &pb, char *errbuf, size_t errlen);
+cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,
+                           const PredProg *progs, const double *consts, int P,
+                           uint32_t *bitmaps, uint64_t bm_words, unsigned long long *popcnt,
+                           int sm_count, cudaStream_t st);
+
+// ---- exact FP32 scan (scan_f32.cu)
+struct ScanF32Args {
+    const float *__restrict__ vecs;
+    uint64_t nrows;
+    int dpad;
+    const float *__restrict__ queries;  // [nq][dpad]
+    int nq;
+    const uint32_t *__restrict__ bitmaps;  // [P][bm_words]
+    uint64_t bm_words;
+    const int32_t *__restrict__ qprog;  // [nq]
+    int K, S, CB;
+    uint64_t rows_per_cta;  // multiple of 32
+    int grow;               // CTAs along the rows
+    int qtiles;
+    unsigned long long *tau;  // [nq]
+    uint64_t *part;           // [nq][grow][K]
+    uint32_t *part_cnt;       // [nq][grow]
+};
+
+struct ScanPlan {
+    int QT, DCH, S, CB, grow, qtiles;
+    uint64_t rows_per_cta;
+    size_t smem;
+    int M;  // merge buffer (keys)
+    size_t merge_smem;
+};
+
+int scan_f32_max_qt(int dim);
+bool plan_scan_f32(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPlan &pl);
+cudaError_t launch_scan_f32(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st);
+cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int grow, int K,
+                         const ScanPlan &pl, const unsigned long long *tau,
+                         const int32_t *qprog, const unsigned long long *popcnt,
+                         uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
+                         uint8_t *trunc, cudaStream_t st);
+
+// ---- batch staging (brute.cu)
+struct DevBatch {
+    Buf *stage_h = nullptr;
+    Buf *stage_d = nullptr;
+    int nq = 0, P = 0;
+    size_t off_q = 0, off_qprog = 0, off_progs = 0, off_insns = 0, off_consts = 0, off_extra = 0;
+    size_t bytes = 0;
+};
+
+int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                  DevBatch &db, size_t extra_bytes, char *errbuf, size_t errlen);
+int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen);
+// ev (optional): 5 events recorded before bitmaps, before scan, after scan,
+// after re-rank and after merge.
+int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
+                 uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
+                 cudaEvent_t *ev = nullptr);
+int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                   uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt,
+                   uint8_t *truncated, char *errbuf, size_t errlen);
+
+// ---- graph search (graph.cu)
+int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
+                   const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,
+                   uint32_t *out_cnt, uint8_t *exhausted, char *errbuf, size_t errlen);
+
+}  // namespace pv
