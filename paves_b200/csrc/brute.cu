@@ -88,7 +88,15 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
-    (void)mode;
+    if (mode == 1 && tc_supported(g) && tc_superset(topb) > 0) {
+        if (launch_scan_tc(g, nq, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
+                           s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
+                           errbuf, errlen))
+            return -1;
+        if (ev) cudaEventRecord(ev[4], g->stream);
+        return 0;
+    }
+    g->tc_err = nullptr;
 
     ScanPlan pl;
     if (!plan_scan_f32(g->count, g->dpad, nq, (int)topb, g->sm_count, pl)) {
@@ -195,6 +203,7 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
     PV_CUDA_OK(cudaMemcpyAsync(g->scan.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream),
                errbuf, errlen);
     PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    if (check_tc_watchdog(g, errbuf, errlen)) return -1;
     cudaEventElapsedTime(&g->last_kernel_ms, g->ev0, g->ev1);
     const char *oh = g->scan.out_h.as<char>();
     const uint32_t *cnt = (const uint32_t *)(oh + off_cnt);

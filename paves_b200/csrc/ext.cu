@@ -99,6 +99,7 @@ extern "C" int pv_batch_run(PvBatch *b, int iters, float *stage_ms, float *total
                              errlen, b->ev))
                 return -1;
             PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+            if (check_tc_watchdog(g, errbuf, errlen)) return -1;
             for (int s = 0; s < 4; s++) {
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, b->ev[s], b->ev[s + 1]);
@@ -116,6 +117,7 @@ extern "C" int pv_batch_run(PvBatch *b, int iters, float *stage_ms, float *total
                 return -1;
         cudaEventRecord(b->ev[4], g->stream);
         PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+        if (check_tc_watchdog(g, errbuf, errlen)) return -1;
         cudaEventElapsedTime(&tot, b->ev[0], b->ev[4]);
     }
     if (total_ms) *total_ms = tot;

@@ -194,7 +194,9 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
     if (l0 && l0_stride < 2) return fail("bad l0 stride", cudaSuccess);
 
     const int dpad = (dim + 3) & ~3;
-    const int kpad = (dim + 63) & ~63;
+    // low-precision row stride: whole 128-byte swizzle rows
+    const int kpad = precision == FV_GPU_PREC_FP8 ? (dim + 127) & ~127 : (dim + 63) & ~63;
+    const uint64_t rows_pad = (count + 127) & ~127ull;  // norms/scales per 128-row tile
     size_t need = count * (size_t)dpad * 4 + count * (size_t)ncols * 12;
     if (l0) need += count * (size_t)(l0_stride - 1) * 4 + count * 2;
     if (precision != FV_GPU_PREC_FP32) need += count * (size_t)kpad * 2 + count * 8;
@@ -272,10 +274,13 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         const size_t esz = f8 ? 1 : 2;
         if ((e = cudaMalloc(&g->d_vlow, count * (size_t)kpad * esz)) != cudaSuccess)
             return bail("low-precision rows", e);
-        if ((e = cudaMalloc(&g->d_norm, count * 4)) != cudaSuccess) return bail("norms", e);
+        if ((e = cudaMalloc(&g->d_norm, rows_pad * 4)) != cudaSuccess) return bail("norms", e);
+        if ((e = cudaMemset(g->d_norm, 0, rows_pad * 4)) != cudaSuccess) return bail("norms", e);
         unsigned blocks = (unsigned)((count + 7) / 8);
         if (f8) {
-            if ((e = cudaMalloc(&g->d_vscale, count * 4)) != cudaSuccess)
+            if ((e = cudaMalloc(&g->d_vscale, rows_pad * 4)) != cudaSuccess)
+                return bail("scales", e);
+            if ((e = cudaMemset(g->d_vscale, 0, rows_pad * 4)) != cudaSuccess)
                 return bail("scales", e);
             to_fp8_kernel<<<blocks, 256, 0, g->stream>>>(g->d_vecs, dpad, dim, count,
                                                          (__nv_fp8_e4m3 *)g->d_vlow, kpad,

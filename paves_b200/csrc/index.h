@@ -103,6 +103,7 @@ struct FvGpuIndex {
 
     pv::ScanScratch scan;
     pv::GraphScratch graph;
+    int *tc_err = nullptr;  // watchdog word of the last tensor-core scan (device)
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels
     std::vector<uint32_t> graph_stats;  // last graph batch: [nq][4] counters
 };

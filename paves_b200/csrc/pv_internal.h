@@ -72,6 +72,18 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
                    uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt,
                    uint8_t *truncated, char *errbuf, size_t errlen);
 
+// ---- tensor-core scan (scan_tc.cu)
+int tc_superset(uint32_t topb);
+bool tc_supported(const FvGpuIndex *g);
+int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qprog,
+                   const uint32_t *bitmaps, uint64_t bm_words,
+                   const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
+                   uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
+                   size_t errlen);
+// Reads and clears the watchdog word of the last tensor-core scan after the
+// stream was synchronized; -1 + errbuf if a bounded wait expired.
+int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);
+
 // ---- graph search (graph.cu)
 int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
                    const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,

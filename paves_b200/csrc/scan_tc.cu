@@ -1,0 +1,578 @@
+// scan_tc.cu — reduced-precision filtered L2 scan on the 5th-gen tensor
+// cores (tcgen05, TMEM accumulators, TMA-fed shared memory).
+//
+// New path beside the exact scan (the reference has no tensor-core path;
+// its approximate SQ8 scan is gpu_engine.cu:759-893 + rerank :934-992).
+// Distances use the norm form ||x||^2 + ||q||^2 - 2 q.x with the dot
+// products from one GEMM per 128-row tile:
+//     D[128 queries][128 rows] = Q[128 x K] * X_tile[128 x K]^T
+// (A = query tile, resident in shared memory; B = row tile, streamed by
+// TMA in 128-byte-swizzled K-major boxes). D lives in TMEM, double
+// buffered, so the MMA of tile t+1 overlaps the epilogue of tile t.
+// In TMEM, lane = query and column = row: each epilogue thread owns ONE
+// query, walks the tile's 128 rows and keeps that query's best K' keys
+// in a private shared-memory list with its threshold in a register; the
+// bitmap predicate is read only for rows that beat the threshold. The
+// grid-wide per-query bound in global memory lets CTAs prune with each
+// other's K'-th key. Per-CTA lists are merged per query and the K'
+// survivors re-ranked with exact FP32 distances (rerank_kernel).
+//
+// BF16 operands are exact for integers up to 256, so on integer-valued
+// rows (the benchmark data) every distance is exact; FP8-E4M3 rows carry a
+// per-row scale (absmax / 448) and the query a per-query scale.
+//
+// Warp roles (192 threads): warp 0 TMA producer, warp 1 TMEM allocator +
+// MMA issuer, warps 2-5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).
+// All waits are bounded by a deadline and unwind through an abort flag.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include "pv_internal.h"
+#include "sm100.cuh"
+
+namespace pv {
+
+using namespace sm100;
+
+constexpr int TC_BM = 128;          // queries per tile (MMA M)
+constexpr int TC_BN = 128;          // rows per tile (MMA N)
+constexpr int TC_KB_BYTES = 128;    // bytes of K per swizzle row / TMA box
+constexpr int TC_BOX = TC_BN * TC_KB_BYTES;  // 16 KB per K-block box
+constexpr int TC_KBS = 2;           // K-blocks per pipeline stage
+constexpr int TC_THREADS = 192;
+
+template <bool FP8>
+__device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                              uint32_t acc) {
+    if (FP8) mma_f8(d, a, b, idesc, acc);
+    else mma_f16(d, a, b, idesc, acc);
+}
+
+struct TcArgs {
+    uint64_t nrows;
+    int kblocks;        // K-blocks (128 bytes of K each) per row
+    int nq;
+    int qtiles;
+    int grow;           // CTAs along rows per query tile
+    uint64_t tiles_per_cta;
+    int KP;             // candidates kept per query (K')
+    int NS;             // pipeline stages
+    const float *__restrict__ xnorm;   // [rows padded to 128]
+    const float *__restrict__ xscale;  // fp8: per-row scale, else null
+    const float *__restrict__ qnorm;   // [nqpad]
+    const float *__restrict__ qscale;  // fp8: per-query scale, else null
+    const int32_t *__restrict__ qprog;
+    const uint32_t *__restrict__ bitmaps;
+    uint64_t bm_words;
+    unsigned long long *tau;  // [nq] grid-wide bound
+    uint64_t *part;           // [nq][grow][KP]
+    uint32_t *part_cnt;       // [nq][grow]
+    int *err;
+    uint64_t timeout_ns;
+};
+
+template <bool FP8>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmQ,
+               TcArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte alignment for the swizzled operand tiles
+    unsigned char *base =
+        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int KBt = a.kblocks;
+    const int NS = a.NS;
+    const int KP = a.KP;
+    unsigned char *sQ = base;                                  // KBt boxes
+    unsigned char *sX = sQ + (size_t)KBt * TC_BOX;             // NS * KBS boxes
+    uint64_t *lists = (uint64_t *)(sX + (size_t)NS * TC_KBS * TC_BOX);  // [128][KP]
+    uint64_t *bars = lists + (size_t)TC_BM * KP;
+    uint64_t *full = bars;            // [NS]
+    uint64_t *empty = full + NS;      // [NS]
+    uint64_t *tfull = empty + NS;     // [2]
+    uint64_t *tempty = tfull + 2;     // [2]
+    uint64_t *qbar = tempty + 2;      // [1]
+    uint64_t *done = qbar + 1;        // [1]
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int qtile = blockIdx.x % a.qtiles;
+    const int rgrp = blockIdx.x / a.qtiles;
+    const uint64_t tile0 = (uint64_t)rgrp * a.tiles_per_cta;
+    const uint64_t ntiles_all = (a.nrows + TC_BN - 1) / TC_BN;
+    uint64_t ntiles = tile0 < ntiles_all ? ntiles_all - tile0 : 0;
+    if (ntiles > a.tiles_per_cta) ntiles = a.tiles_per_cta;
+    const int nkc = (KBt + TC_KBS - 1) / TC_KBS;
+    const uint64_t deadline = globaltimer() + a.timeout_ns;
+
+    if (tid == 0) {
+        s_abort = 0;
+        for (int i = 0; i < NS; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], TC_BM);
+        }
+        mbar_init(qbar, 1);
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&s_tmem, 256);
+        tmem_relinquish();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    volatile int *abort_flag = &s_abort;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            prefetch_tmap(&tmX);
+            prefetch_tmap(&tmQ);
+            mbar_arrive_expect_tx(qbar, (uint32_t)KBt * TC_BOX);
+            for (int kb = 0; kb < KBt; kb++)
+                tma_load_2d(sQ + (size_t)kb * TC_BOX, &tmQ, kb * (FP8 ? 128 : 64),
+                            qtile * TC_BM, qbar);
+            uint64_t it = 0;
+            bool ok = true;
+            for (uint64_t t = 0; t < ntiles && ok; t++) {
+                const int y = (int)((tile0 + t) * TC_BN);
+                for (int kc = 0; kc < nkc; kc++, it++) {
+                    const int s = (int)(it % NS);
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if (!mbar_wait(&empty[s], ph ^ 1, deadline, abort_flag)) { ok = false; break; }
+                    const int nkb = min(TC_KBS, KBt - kc * TC_KBS);
+                    mbar_arrive_expect_tx(&full[s], (uint32_t)nkb * TC_BOX);
+                    for (int kb = 0; kb < nkb; kb++)
+                        tma_load_2d(sX + ((size_t)s * TC_KBS + kb) * TC_BOX, &tmX,
+                                    (kc * TC_KBS + kb) * (FP8 ? 128 : 64), y, &full[s]);
+                }
+            }
+            if (!ok) {
+                s_abort = 1;
+                atomicExch(a.err, 1);
+            }
+            // copies still in flight land before the CTA leaves
+            const uint64_t first = it > (uint64_t)NS ? it - NS : 0;
+            const uint64_t d2 = globaltimer() + a.timeout_ns;
+            volatile int zero = 0;
+            for (uint64_t j = first; j < it; j++)
+                mbar_wait(&full[j % NS], (uint32_t)((j / NS) & 1), d2, &zero);
+            mbar_wait(qbar, 0, d2, &zero);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = FP8 ? idesc_make(FMT_E4M3, FMT_E4M3, TC_BM, TC_BN)
+                                       : idesc_make(FMT_BF16, FMT_BF16, TC_BM, TC_BN);
+            bool ok = mbar_wait(qbar, 0, deadline, abort_flag);
+            uint64_t it = 0;
+            for (uint64_t t = 0; t < ntiles && ok; t++) {
+                const int acc = (int)(t & 1);
+                const uint32_t aph = (uint32_t)((t >> 1) & 1);
+                if (!mbar_wait(&tempty[acc], aph ^ 1, deadline, abort_flag)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t dcol = tmem + (uint32_t)acc * TC_BN;
+                for (int kc = 0; kc < nkc && ok; kc++, it++) {
+                    const int s = (int)(it % NS);
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if (!mbar_wait(&full[s], ph, deadline, abort_flag)) { ok = false; break; }
+                    tc_fence_after();
+                    const int nkb = min(TC_KBS, KBt - kc * TC_KBS);
+                    for (int kb = 0; kb < nkb; kb++) {
+                        const uint64_t ad = desc_sw128(sQ + (size_t)(kc * TC_KBS + kb) * TC_BOX);
+                        const uint64_t bd = desc_sw128(sX + ((size_t)s * TC_KBS + kb) * TC_BOX);
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++)  // 4 x 32 bytes of K per block
+                            mma_f16_or_f8<FP8>(dcol, ad + 2 * kk, bd + 2 * kk, idesc,
+                                               (kc | kb | kk) != 0);
+                    }
+                    mma_commit(&empty[s]);
+                }
+                if (ok) mma_commit(&tfull[acc]);
+            }
+            if (!ok) {
+                s_abort = 1;
+                atomicExch(a.err, 2);
+            }
+            // all issued MMAs complete before TMEM is released
+            mma_commit(done);
+            volatile int zero = 0;
+            mbar_wait(done, 0, globaltimer() + a.timeout_ns, &zero);
+        }
+    } else {
+        // ------------------------------------------------ epilogue
+        const int qd = warp & 3;
+        const int m = qd * 32 + lane;  // query slot within the tile
+        const int qg = qtile * TC_BM + m;
+        const bool qvalid = qg < a.nq;
+        const float qn = qvalid ? a.qnorm[qg] : 0.f;
+        const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
+        const int pg = qvalid ? a.qprog[qg] : -1;
+        const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
+        uint64_t *L = lists + (size_t)m * KP;
+        int n = 0, wi = 0;
+        uint64_t lmax = KEY_MAX;   // worst kept key once the list is full
+        uint64_t thr = KEY_MAX;    // admission threshold
+        bool ok = true;
+        for (uint64_t t = 0; t < ntiles; t++) {
+            const int acc = (int)(t & 1);
+            const uint32_t aph = (uint32_t)((t >> 1) & 1);
+            if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) { ok = false; break; }
+            tc_fence_after();
+            const uint64_t rbase = (tile0 + t) * TC_BN;
+            if (qvalid) {
+                const unsigned long long g = *((volatile unsigned long long *)(a.tau + qg));
+                if (g < thr) thr = g;
+            }
+            float xr[4], xs[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                xr[j] = __ldg(a.xnorm + rbase + j * 32 + lane);
+                xs[j] = FP8 ? __ldg(a.xscale + rbase + j * 32 + lane) : 1.f;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                uint32_t r[32];
+                tmem_ld_32x32b_x32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)acc * TC_BN +
+                                       c * 32,
+                                   r);
+                tmem_ld_wait();
+#pragma unroll
+                for (int i = 0; i < 32; i++) {
+                    const float xn = __shfl_sync(0xffffffffu, xr[c], i);
+                    float dot = __uint_as_float(r[i]);
+                    if (FP8) dot *= __shfl_sync(0xffffffffu, xs[c], i) * qs;
+                    float d = fmaf(-2.f, dot, xn + qn);
+                    d = fmaxf(d, 0.f);
+                    const uint64_t row = rbase + c * 32 + i;
+                    const uint64_t key = make_key(d, (uint32_t)row);
+                    if (key < thr && qvalid && row < a.nrows) {
+                        if (!bm || ((__ldg(bm + (row >> 5)) >> (row & 31)) & 1u)) {
+                            if (n < KP) {
+                                L[n++] = key;
+                                if (n == KP) {
+                                    wi = 0;
+                                    for (int j = 1; j < KP; j++)
+                                        if (L[j] > L[wi]) wi = j;
+                                    lmax = L[wi];
+                                    if (lmax < thr) thr = lmax;
+                                }
+                            } else {
+                                L[wi] = key;
+                                wi = 0;
+                                for (int j = 1; j < KP; j++)
+                                    if (L[j] > L[wi]) wi = j;
+                                lmax = L[wi];
+                                if (lmax < thr) thr = lmax;
+                            }
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);
+            if (qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
+        }
+        if (!ok) {
+            s_abort = 1;
+            atomicExch(a.err, 3);
+        }
+        if (qvalid) {
+            // ascending list (insertion sort, <= KP entries)
+            for (int i = 1; i < n; i++) {
+                const uint64_t v = L[i];
+                int j = i - 1;
+                while (j >= 0 && L[j] > v) {
+                    L[j + 1] = L[j];
+                    j--;
+                }
+                L[j + 1] = v;
+            }
+            uint64_t *dst = a.part + ((uint64_t)qg * a.grow + rgrp) * KP;
+            for (int i = 0; i < n; i++) dst[i] = L[i];
+            a.part_cnt[(uint64_t)qg * a.grow + rgrp] = (uint32_t)n;
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 256);
+    }
+}
+
+}  // namespace pv
+
+namespace pv {
+
+// ---------------------------------------------------------------- queries
+// f32 queries [nq][dpad] -> low-precision tile rows [nqpad][row_bytes] with
+// zero padding, plus ||q||^2 of the rounded query (and the fp8 scale).
+__global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad, int dim,
+                                  int nqpad, int kelems, bool fp8, unsigned char *__restrict__ out,
+                                  float *__restrict__ qnorm, float *__restrict__ qscale) {
+    const int lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (qi >= nqpad) return;
+    const bool ok = qi < nq;
+    float amax = 0.f;
+    if (fp8 && ok)
+        for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(q[(size_t)qi * dpad + j]));
+    for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const float s = amax > 0.f ? amax / 448.f : 1.f;
+    float acc = 0.f;
+    for (int j = lane; j < kelems; j += 32) {
+        const float v = (ok && j < dim) ? q[(size_t)qi * dpad + j] : 0.f;
+        float r;
+        if (fp8) {
+            __nv_fp8_e4m3 b(v / s);
+            out[(size_t)qi * kelems + j] = *(unsigned char *)&b;
+            r = float(b) * s;
+        } else {
+            __nv_bfloat16 b = __float2bfloat16_rn(v);
+            ((__nv_bfloat16 *)out)[(size_t)qi * kelems + j] = b;
+            r = __bfloat162float(b);
+        }
+        acc = fmaf(r, r, acc);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        qnorm[qi] = acc;
+        if (qscale) qscale[qi] = s;
+    }
+}
+
+// ---------------------------------------------------------------- re-rank
+// Exact FP32 distances (difference form) for each query's K' merged
+// candidates; keeps the best topb by (dist, id). One CTA (4 warps) per query.
+__global__ void __launch_bounds__(128)
+rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict__ queries,
+              const FvHit *__restrict__ cand, const uint32_t *__restrict__ cand_cnt, int KP,
+              uint32_t topb, const int32_t *__restrict__ qprog,
+              const unsigned long long *__restrict__ popcnt, uint64_t nrows,
+              FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
+              uint8_t *__restrict__ trunc) {
+    __shared__ uint64_t keys[64];
+    const int q = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int n = (int)cand_cnt[q];
+    if (n > KP) n = KP;
+    const float *qv = queries + (size_t)q * dpad;
+    for (int j = warp; j < n; j += 4) {
+        const uint32_t row = (uint32_t)cand[(size_t)q * KP + j].node;
+        const float *x = vecs + (size_t)row * dpad;
+        float acc = 0.f;
+        for (int k = lane * 4; k < dpad; k += 128) {
+            float4 v = __ldg((const float4 *)(x + k));
+            float4 w = __ldg((const float4 *)(qv + k));
+            float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
+            acc = fmaf(d0, d0, acc);
+            acc = fmaf(d1, d1, acc);
+            acc = fmaf(d2, d2, acc);
+            acc = fmaf(d3, d3, acc);
+        }
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) keys[j] = make_key(acc, row);
+    }
+    __syncthreads();
+    // rank placement (keys are unique): position = number of smaller keys
+    uint64_t mine = 0;
+    int rank = 0;
+    if ((int)threadIdx.x < n) {
+        mine = keys[threadIdx.x];
+        for (int j = 0; j < n; j++) rank += keys[j] < mine;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < n && rank < (int)topb) {
+        FvHit h;
+        h.node = key_row(mine);
+        h.dist = key_dist(mine);
+        out[(size_t)q * topb + rank] = h;
+    }
+    if (threadIdx.x == 0) {
+        out_cnt[q] = (uint32_t)(n < (int)topb ? n : (int)topb);
+        const int pg = qprog[q];
+        const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
+        trunc[q] = passing > (unsigned long long)topb ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------- host side
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) ==
+                cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 2-D row-major [rows][inner] tensor map with 128-byte swizzled boxes of
+// [128 rows][128 bytes].
+static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner, uint64_t rows) {
+    auto enc = get_encode();
+    if (!enc) return false;
+    const uint32_t esz = fp8 ? 1 : 2;
+    cuuint64_t dims[2] = {inner, rows};
+    cuuint64_t strides[1] = {inner * esz};
+    cuuint32_t box[2] = {TC_KB_BYTES / esz, TC_BN};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     const_cast<void *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+int tc_superset(uint32_t topb) {
+    int kp = 4 * (int)topb;
+    if (kp > 64) kp = 64;
+    if (kp < (int)topb) return 0;  // topb beyond the superset capacity
+    return kp;
+}
+
+bool tc_supported(const FvGpuIndex *g) {
+    if (g->precision == FV_GPU_PREC_FP32 || !g->d_vlow) return false;
+    const int row_bytes = g->kpad * (g->precision == FV_GPU_PREC_FP8 ? 1 : 2);
+    return row_bytes <= 512;  // query tile <= 64 KB of shared memory
+}
+
+static size_t tc_smem(int kblocks, int NS, int KP) {
+    return 1024 + (size_t)kblocks * TC_BOX + (size_t)NS * TC_KBS * TC_BOX +
+           (size_t)TC_BM * KP * 8 + (size_t)(2 * NS + 6) * 8;
+}
+
+// Launches query prep, the tensor-core scan, the per-query merge and the
+// exact re-rank. Inputs: f32 queries [nq][dpad] on the device, predicate
+// programs/bitmaps already built.
+int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qprog,
+                   const uint32_t *bitmaps, uint64_t bm_words,
+                   const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
+                   uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
+                   size_t errlen) {
+    const bool fp8 = g->precision == FV_GPU_PREC_FP8;
+    const int esz = fp8 ? 1 : 2;
+    const int kblocks = g->kpad * esz / TC_KB_BYTES;
+    const int KP = tc_superset(topb);
+    if (!KP || !tc_supported(g)) {
+        snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
+        return -1;
+    }
+    int NS = 4;
+    while (NS > 2 && tc_smem(kblocks, NS, KP) > 227 * 1024) NS--;
+    const size_t smem = tc_smem(kblocks, NS, KP);
+    const int qtiles = (nq + TC_BM - 1) / TC_BM;
+    const int nqpad = qtiles * TC_BM;
+    const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;
+    int grow = g->sm_count / qtiles;
+    if (grow < 1) grow = 1;
+    uint64_t maxg = (ntiles_all + 3) / 4;
+    if ((uint64_t)grow > maxg) grow = (int)maxg;
+    const uint64_t tpc = (ntiles_all + grow - 1) / grow;
+    grow = (int)((ntiles_all + tpc - 1) / tpc);
+
+    ScanScratch &s = g->scan;
+    const size_t qbytes = (size_t)nqpad * g->kpad * esz;
+    const size_t off_qn = (qbytes + 255) & ~(size_t)255;
+    const size_t off_qs = off_qn + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
+    const size_t off_err = off_qs + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
+    const size_t off_cand = off_err + 256;
+    const size_t off_ccnt = off_cand + (((size_t)nq * KP * sizeof(FvHit) + 255) & ~(size_t)255);
+    const size_t off_ctr = off_ccnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
+    const size_t cbytes = off_ctr + (size_t)nq + 256;
+    PV_CUDA_OK(s.cand.ensure(cbytes), errbuf, errlen);
+    PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
+    PV_CUDA_OK(s.part.ensure((size_t)nq * grow * KP * 8), errbuf, errlen);
+    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * grow * 4), errbuf, errlen);
+    unsigned char *c = s.cand.as<unsigned char>();
+    int *d_err = (int *)(c + off_err);
+    PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
+    PV_CUDA_OK(cudaMemsetAsync(d_err, 0, 4, g->stream), errbuf, errlen);
+
+    query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
+        d_q, nq, g->dpad, g->dim, nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
+        fp8 ? (float *)(c + off_qs) : nullptr);
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+
+    CUtensorMap tmX, tmQ;
+    if (!make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count) ||
+        !make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
+        snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
+        return -1;
+    }
+    TcArgs a;
+    a.nrows = g->count;
+    a.kblocks = kblocks;
+    a.nq = nq;
+    a.qtiles = qtiles;
+    a.grow = grow;
+    a.tiles_per_cta = tpc;
+    a.KP = KP;
+    a.NS = NS;
+    a.xnorm = g->d_norm;
+    a.xscale = fp8 ? g->d_vscale : nullptr;
+    a.qnorm = (const float *)(c + off_qn);
+    a.qscale = fp8 ? (const float *)(c + off_qs) : nullptr;
+    a.qprog = d_qprog;
+    a.bitmaps = bitmaps;
+    a.bm_words = bm_words;
+    a.tau = s.tau.as<unsigned long long>();
+    a.part = s.part.as<uint64_t>();
+    a.part_cnt = s.part_cnt.as<uint32_t>();
+    a.err = d_err;
+    a.timeout_ns = 2000000000ull;
+    if (ev) cudaEventRecord(ev[1], g->stream);
+    if (fp8) {
+        PV_CUDA_OK(cudaFuncSetAttribute(scan_tc_kernel<true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                   errbuf, errlen);
+        scan_tc_kernel<true><<<grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ, a);
+    } else {
+        PV_CUDA_OK(cudaFuncSetAttribute(scan_tc_kernel<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                   errbuf, errlen);
+        scan_tc_kernel<false><<<grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ, a);
+    }
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    if (ev) cudaEventRecord(ev[2], g->stream);
+    ScanPlan pl;
+    pl.M = 1024;
+    pl.merge_smem = (size_t)pl.M * 8 + (size_t)grow * 8;
+    FvHit *cand = (FvHit *)(c + off_cand);
+    uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
+    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, grow, KP, pl, a.tau, d_qprog, popcnt, g->count,
+                            nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream),
+               errbuf, errlen);
+    rerank_kernel<<<nq, 128, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, KP, topb,
+                                             d_qprog, popcnt, g->count, d_out, d_cnt, d_trunc);
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    if (ev) cudaEventRecord(ev[3], g->stream);
+    g->tc_err = d_err;
+    return 0;
+}
+
+}  // namespace pv
+
+namespace pv {
+int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen) {
+    if (!g->tc_err) return 0;
+    int e = 0;
+    PV_CUDA_OK(cudaMemcpy(&e, g->tc_err, 4, cudaMemcpyDeviceToHost), errbuf, errlen);
+    if (e) {
+        cudaMemset(g->tc_err, 0, 4);
+        snprintf(errbuf, errlen, "gpu: tensor-core scan wait expired (role %d)", e);
+        return -1;
+    }
+    return 0;
+}
+}  // namespace pv
