@@ -49,7 +49,8 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          const ScanPlan &pl, const unsigned long long *tau,
                          const int32_t *qprog, const unsigned long long *popcnt,
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
-                         uint8_t *trunc, cudaStream_t st);
+                         uint8_t *trunc, cudaStream_t st,
+                         unsigned long long *tau_out = nullptr);
 
 // ---- batch staging (brute.cu)
 struct DevBatch {

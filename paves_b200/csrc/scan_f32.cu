@@ -202,7 +202,7 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
              const int32_t *__restrict__ qprog,
              const unsigned long long *__restrict__ popcnt, uint64_t nrows,
              FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
-             uint8_t *__restrict__ trunc) {
+             uint8_t *__restrict__ trunc, unsigned long long *__restrict__ tau_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *buf = (uint64_t *)smem_raw;   // [M]
     int *s_c = (int *)(buf + M);            // [grow] prefix lengths
@@ -283,6 +283,8 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
         const int pg = qprog[q];
         const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
         trunc[q] = passing > (unsigned long long)K ? 1 : 0;
+        // the K-th merged key bounds the K-th key of any superset of rows
+        if (tau_out && lo == K) tau_out[q] = buf[K - 1];
     }
 }
 
@@ -384,12 +386,12 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          const ScanPlan &pl, const unsigned long long *tau,
                          const int32_t *qprog, const unsigned long long *popcnt,
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
-                         uint8_t *trunc, cudaStream_t st) {
+                         uint8_t *trunc, cudaStream_t st, unsigned long long *tau_out) {
     cudaError_t e = cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)pl.merge_smem);
     if (e != cudaSuccess) return e;
     merge_kernel<<<nq, 256, pl.merge_smem, st>>>(part, part_cnt, grow, K, pl.M, tau, qprog,
-                                                 popcnt, nrows, out, out_cnt, trunc);
+                                                 popcnt, nrows, out, out_cnt, trunc, tau_out);
     return cudaGetLastError();
 }
 

@@ -57,6 +57,8 @@ struct TcArgs {
     int qtiles;
     int grow;           // CTAs along rows per query tile
     uint64_t tiles_per_cta;
+    uint64_t tile0_mul;  // first tile of CTA group g = g * tile0_mul
+    uint64_t tile_step;  // stride between a CTA's tiles
     int KP;             // candidates kept per query (K')
     int NS;             // pipeline stages
     const float *__restrict__ xnorm;   // [rows padded to 128]
@@ -100,9 +102,11 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int qtile = blockIdx.x % a.qtiles;
     const int rgrp = blockIdx.x / a.qtiles;
-    const uint64_t tile0 = (uint64_t)rgrp * a.tiles_per_cta;
+    // this CTA's tiles: tile0 + t * tile_step, t < ntiles
+    const uint64_t tile0 = (uint64_t)rgrp * a.tile0_mul;
     const uint64_t ntiles_all = (a.nrows + TC_BN - 1) / TC_BN;
-    uint64_t ntiles = tile0 < ntiles_all ? ntiles_all - tile0 : 0;
+    uint64_t ntiles =
+        tile0 < ntiles_all ? (ntiles_all - tile0 + a.tile_step - 1) / a.tile_step : 0;
     if (ntiles > a.tiles_per_cta) ntiles = a.tiles_per_cta;
     const int nkc = (KBt + TC_KBS - 1) / TC_KBS;
     const uint64_t deadline = globaltimer() + a.timeout_ns;
@@ -142,7 +146,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             uint64_t it = 0;
             bool ok = true;
             for (uint64_t t = 0; t < ntiles && ok; t++) {
-                const int y = (int)((tile0 + t) * TC_BN);
+                const int y = (int)((tile0 + t * a.tile_step) * TC_BN);
                 for (int kc = 0; kc < nkc; kc++, it++) {
                     const int s = (int)(it % NS);
                     const uint32_t ph = (uint32_t)((it / NS) & 1);
@@ -216,20 +220,27 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
         const int pg = qvalid ? a.qprog[qg] : -1;
         const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
-        uint64_t *L = lists + (size_t)m * KP;
+        // thread-private list, interleaved [KP][128] so a warp's accesses to
+        // the same slot index hit 32 different banks
+        uint64_t *L = lists + m;
+#define PV_L(j) L[(size_t)(j) * TC_BM]
         int n = 0, wi = 0;
         uint64_t lmax = KEY_MAX;   // worst kept key once the list is full
-        uint64_t thr = KEY_MAX;    // admission threshold
+        uint64_t thr = qvalid ? KEY_MAX : 0ull;  // admission threshold
+        float thr_d = qvalid ? __int_as_float(0x7f800000) : -1.f;  // its distance
         bool ok = true;
         for (uint64_t t = 0; t < ntiles; t++) {
             const int acc = (int)(t & 1);
             const uint32_t aph = (uint32_t)((t >> 1) & 1);
             if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) { ok = false; break; }
             tc_fence_after();
-            const uint64_t rbase = (tile0 + t) * TC_BN;
+            const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN;
             if (qvalid) {
                 const unsigned long long g = *((volatile unsigned long long *)(a.tau + qg));
-                if (g < thr) thr = g;
+                if (g < thr) {
+                    thr = g;
+                    thr_d = key_dist(g);
+                }
             }
             float xr[4], xs[4];
 #pragma unroll
@@ -251,26 +262,36 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     if (FP8) dot *= __shfl_sync(0xffffffffu, xs[c], i) * qs;
                     float d = fmaf(-2.f, dot, xn + qn);
                     d = fmaxf(d, 0.f);
-                    const uint64_t row = rbase + c * 32 + i;
-                    const uint64_t key = make_key(d, (uint32_t)row);
-                    if (key < thr && qvalid && row < a.nrows) {
-                        if (!bm || ((__ldg(bm + (row >> 5)) >> (row & 31)) & 1u)) {
+                    if (d <= thr_d) {
+                        const uint64_t row = rbase + c * 32 + i;
+                        const uint64_t key = make_key(d, (uint32_t)row);
+                        // <= : the seeded bound is itself a row key that
+                        // this pass must admit again (keys are unique)
+                        if (key <= thr && row < a.nrows &&
+                            (!bm || ((__ldg(bm + (row >> 5)) >> (row & 31)) & 1u))) {
                             if (n < KP) {
-                                L[n++] = key;
+                                PV_L(n) = key;
+                                n++;
                                 if (n == KP) {
                                     wi = 0;
                                     for (int j = 1; j < KP; j++)
-                                        if (L[j] > L[wi]) wi = j;
-                                    lmax = L[wi];
-                                    if (lmax < thr) thr = lmax;
+                                        if (PV_L(j) > PV_L(wi)) wi = j;
+                                    lmax = PV_L(wi);
+                                    if (lmax < thr) {
+                                        thr = lmax;
+                                        thr_d = key_dist(lmax);
+                                    }
                                 }
                             } else {
-                                L[wi] = key;
+                                PV_L(wi) = key;
                                 wi = 0;
                                 for (int j = 1; j < KP; j++)
-                                    if (L[j] > L[wi]) wi = j;
-                                lmax = L[wi];
-                                if (lmax < thr) thr = lmax;
+                                    if (PV_L(j) > PV_L(wi)) wi = j;
+                                lmax = PV_L(wi);
+                                if (lmax < thr) {
+                                    thr = lmax;
+                                    thr_d = key_dist(lmax);
+                                }
                             }
                         }
                     }
@@ -287,18 +308,19 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         if (qvalid) {
             // ascending list (insertion sort, <= KP entries)
             for (int i = 1; i < n; i++) {
-                const uint64_t v = L[i];
+                const uint64_t v = PV_L(i);
                 int j = i - 1;
-                while (j >= 0 && L[j] > v) {
-                    L[j + 1] = L[j];
+                while (j >= 0 && PV_L(j) > v) {
+                    PV_L(j + 1) = PV_L(j);
                     j--;
                 }
-                L[j + 1] = v;
+                PV_L(j + 1) = v;
             }
             uint64_t *dst = a.part + ((uint64_t)qg * a.grow + rgrp) * KP;
-            for (int i = 0; i < n; i++) dst[i] = L[i];
+            for (int i = 0; i < n; i++) dst[i] = PV_L(i);
             a.part_cnt[(uint64_t)qg * a.grow + rgrp] = (uint32_t)n;
         }
+#undef PV_L
     }
     __syncthreads();
     if (warp == 1) {
@@ -531,25 +553,46 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     a.part_cnt = s.part_cnt.as<uint32_t>();
     a.err = d_err;
     a.timeout_ns = 2000000000ull;
+    PV_CUDA_OK(cudaFuncSetAttribute(fp8 ? (const void *)scan_tc_kernel<true>
+                                        : (const void *)scan_tc_kernel<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               errbuf, errlen);
+    auto run = [&](const TcArgs &args) {
+        if (fp8)
+            scan_tc_kernel<true><<<args.grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ,
+                                                                                     args);
+        else
+            scan_tc_kernel<false><<<args.grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ,
+                                                                                      args);
+        return cudaGetLastError();
+    };
+    FvHit *cand = (FvHit *)(c + off_cand);
+    uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
     if (ev) cudaEventRecord(ev[1], g->stream);
-    if (fp8) {
-        PV_CUDA_OK(cudaFuncSetAttribute(scan_tc_kernel<true>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+    // Seeding pass: one tile per CTA from an evenly strided sample; the
+    // merged K'-th key of the sample bounds the K'-th key of the whole
+    // scan, so the main pass admits only rows that can still matter.
+    if (ntiles_all >= 8 * (uint64_t)grow) {
+        TcArgs sa = a;
+        sa.tile0_mul = ntiles_all / grow;
+        sa.tile_step = 1;
+        sa.tiles_per_cta = 1;
+        PV_CUDA_OK(run(sa), errbuf, errlen);
+        ScanPlan sp;
+        sp.M = 1024;
+        sp.merge_smem = (size_t)sp.M * 8 + (size_t)grow * 8;
+        PV_CUDA_OK(launch_merge(a.part, a.part_cnt, grow, KP, sp, a.tau, d_qprog, popcnt,
+                                g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
+                                a.tau),
                    errbuf, errlen);
-        scan_tc_kernel<true><<<grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ, a);
-    } else {
-        PV_CUDA_OK(cudaFuncSetAttribute(scan_tc_kernel<false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                   errbuf, errlen);
-        scan_tc_kernel<false><<<grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ, a);
     }
-    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    a.tile0_mul = tpc;
+    a.tile_step = 1;
+    PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
     ScanPlan pl;
     pl.M = 1024;
     pl.merge_smem = (size_t)pl.M * 8 + (size_t)grow * 8;
-    FvHit *cand = (FvHit *)(c + off_cand);
-    uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
     PV_CUDA_OK(launch_merge(a.part, a.part_cnt, grow, KP, pl, a.tau, d_qprog, popcnt, g->count,
                             nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream),
                errbuf, errlen);
