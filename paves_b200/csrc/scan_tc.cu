@@ -41,7 +41,6 @@ constexpr int TC_BN = 128;          // rows per tile (MMA N)
 constexpr int TC_KB_BYTES = 128;    // bytes of K per swizzle row / TMA box
 constexpr int TC_BOX = TC_BN * TC_KB_BYTES;  // 16 KB per K-block box
 constexpr int TC_KBS = 2;           // K-blocks per pipeline stage
-constexpr int TC_THREADS = 192;
 
 template <bool FP8>
 __device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
@@ -73,23 +72,30 @@ struct TcArgs {
     uint32_t *part_cnt;       // [nq][grow]
     int *err;
     uint64_t timeout_ns;
+    // optional per-tile timestamps of CTA 0 (globaltimer ns):
+    // [t][0] stage issued, [t][1] MMA issued, [t][2] epilogue start, [t][3] end
+    uint64_t *trace;
+    int trace_tiles;
 };
 
-template <bool FP8>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+template <bool FP8, int EPI>
+__global__ void __launch_bounds__(64 + 128 * EPI, 1)
 scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmQ,
                TcArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled operand tiles
-    unsigned char *base =
-        (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    // (offset arithmetic on the shared array keeps the shared address space
+    // visible to the compiler: LDS/STS instead of generic accesses)
+    unsigned char *base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int KBt = a.kblocks;
     const int NS = a.NS;
     const int KP = a.KP;
     unsigned char *sQ = base;                                  // KBt boxes
     unsigned char *sX = sQ + (size_t)KBt * TC_BOX;             // NS * KBS boxes
-    uint64_t *lists = (uint64_t *)(sX + (size_t)NS * TC_KBS * TC_BOX);  // [128][KP]
-    uint64_t *bars = lists + (size_t)TC_BM * KP;
+    // per (query, row half) lists [KP][128*EPI] and candidate staging [32][128*EPI]
+    uint64_t *lists = (uint64_t *)(sX + (size_t)NS * TC_KBS * TC_BOX);
+    float *stage = (float *)(lists + (size_t)TC_BM * EPI * KP);
+    uint64_t *bars = (uint64_t *)(stage + 32 * TC_BM * EPI);
     uint64_t *full = bars;            // [NS]
     uint64_t *empty = full + NS;      // [NS]
     uint64_t *tfull = empty + NS;     // [2]
@@ -119,7 +125,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(&tfull[i], 1);
-            mbar_init(&tempty[i], TC_BM);
+            mbar_init(&tempty[i], TC_BM * EPI);
         }
         mbar_init(qbar, 1);
         mbar_init(done, 1);
@@ -157,6 +163,8 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                         tma_load_2d(sX + ((size_t)s * TC_KBS + kb) * TC_BOX, &tmX,
                                     (kc * TC_KBS + kb) * (FP8 ? 128 : 64), y, &full[s]);
                 }
+                if (a.trace && blockIdx.x == 0 && t < (uint64_t)a.trace_tiles)
+                    a.trace[t * 4 + 0] = globaltimer();
             }
             if (!ok) {
                 s_abort = 1;
@@ -200,6 +208,8 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     mma_commit(&empty[s]);
                 }
                 if (ok) mma_commit(&tfull[acc]);
+                if (a.trace && blockIdx.x == 0 && t < (uint64_t)a.trace_tiles)
+                    a.trace[t * 4 + 1] = globaltimer();
             }
             if (!ok) {
                 s_abort = 1;
@@ -212,94 +222,134 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------ epilogue
+        // EPI warps per TMEM lane quadrant: warp w serves the queries of lanes
+        // 32*(w%4).. and the row half (w-2)/4 of every tile.
+        constexpr int CPH = 4 / EPI;         // 32-row chunks per half
+        constexpr int NSLOT = TC_BM * EPI;   // list / stage slots
         const int qd = warp & 3;
-        const int m = qd * 32 + lane;  // query slot within the tile
+        const int half = (warp - 2) >> 2;
+        const int m = qd * 32 + lane;        // query slot within the tile
+        const int slot = half * TC_BM + m;
         const int qg = qtile * TC_BM + m;
         const bool qvalid = qg < a.nq;
         const float qn = qvalid ? a.qnorm[qg] : 0.f;
         const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
         const int pg = qvalid ? a.qprog[qg] : -1;
         const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
-        // thread-private list, interleaved [KP][128] so a warp's accesses to
+        // thread-private list, interleaved [KP][NSLOT] so a warp's accesses to
         // the same slot index hit 32 different banks
-        uint64_t *L = lists + m;
-#define PV_L(j) L[(size_t)(j) * TC_BM]
+        uint64_t *L = lists + slot;
+#define PV_L(j) L[(size_t)(j) * NSLOT]
         int n = 0, wi = 0;
         uint64_t lmax = KEY_MAX;   // worst kept key once the list is full
         uint64_t thr = qvalid ? KEY_MAX : 0ull;  // admission threshold
         float thr_d = qvalid ? __int_as_float(0x7f800000) : -1.f;  // its distance
         bool ok = true;
+        // per-tile inputs, loaded one tile ahead: row norms (and fp8 scales),
+        // predicate words of the 32-row chunks, the grid-wide bound
+        float xr[CPH], xs[CPH];
+        uint32_t bw[CPH];
+        unsigned long long gt = KEY_MAX;
+        auto load_tile = [&](uint64_t tt, float (&x)[CPH], float (&s)[CPH], uint32_t (&w)[CPH],
+                             unsigned long long &g) {
+            const uint64_t rb = (tile0 + tt * a.tile_step) * TC_BN + half * (TC_BN / EPI);
+#pragma unroll
+            for (int j = 0; j < CPH; j++) {
+                x[j] = __ldg(a.xnorm + rb + j * 32 + lane);
+                s[j] = FP8 ? __ldg(a.xscale + rb + j * 32 + lane) : 1.f;
+                const uint64_t r0 = rb + j * 32;
+                uint32_t v = 0;
+                if (r0 < a.nrows) {
+                    v = bm ? __ldg(bm + (r0 >> 5)) : 0xFFFFFFFFu;
+                    if (a.nrows - r0 < 32) v &= (1u << (a.nrows - r0)) - 1u;
+                }
+                w[j] = v;
+            }
+            g = qvalid ? *((volatile unsigned long long *)(a.tau + qg)) : KEY_MAX;
+        };
+        if (ntiles) load_tile(0, xr, xs, bw, gt);
         for (uint64_t t = 0; t < ntiles; t++) {
             const int acc = (int)(t & 1);
             const uint32_t aph = (uint32_t)((t >> 1) & 1);
+            float nxr[CPH], nxs[CPH];
+            uint32_t nbw[CPH];
+            unsigned long long ngt = KEY_MAX;
+            if (t + 1 < ntiles) load_tile(t + 1, nxr, nxs, nbw, ngt);
             if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) { ok = false; break; }
             tc_fence_after();
-            const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN;
-            if (qvalid) {
-                const unsigned long long g = *((volatile unsigned long long *)(a.tau + qg));
-                if (g < thr) {
-                    thr = g;
-                    thr_d = key_dist(g);
-                }
-            }
-            float xr[4], xs[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                xr[j] = __ldg(a.xnorm + rbase + j * 32 + lane);
-                xs[j] = FP8 ? __ldg(a.xscale + rbase + j * 32 + lane) : 1.f;
+            const bool tr = a.trace && blockIdx.x == 0 && slot == 0 && t < (uint64_t)a.trace_tiles;
+            if (tr) a.trace[t * 4 + 2] = globaltimer();
+            const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN + half * (TC_BN / EPI);
+            if (gt < thr) {
+                thr = gt;
+                thr_d = key_dist(gt);
             }
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
+            for (int c = 0; c < CPH; c++) {
                 uint32_t r[32];
                 tmem_ld_32x32b_x32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)acc * TC_BN +
-                                       c * 32,
+                                       half * (TC_BN / EPI) + c * 32,
                                    r);
                 tmem_ld_wait();
+                // hot loop: distances and a candidate mask only; the rare
+                // admissions run below, outside the unrolled code (a negative
+                // norm-form value is clamped there)
+                uint32_t cmask = 0;
 #pragma unroll
                 for (int i = 0; i < 32; i++) {
                     const float xn = __shfl_sync(0xffffffffu, xr[c], i);
                     float dot = __uint_as_float(r[i]);
                     if (FP8) dot *= __shfl_sync(0xffffffffu, xs[c], i) * qs;
-                    float d = fmaf(-2.f, dot, xn + qn);
-                    d = fmaxf(d, 0.f);
+                    const float d = fmaf(-2.f, dot, xn + qn);
                     if (d <= thr_d) {
-                        const uint64_t row = rbase + c * 32 + i;
-                        const uint64_t key = make_key(d, (uint32_t)row);
-                        // <= : the seeded bound is itself a row key that
-                        // this pass must admit again (keys are unique)
-                        if (key <= thr && row < a.nrows &&
-                            (!bm || ((__ldg(bm + (row >> 5)) >> (row & 31)) & 1u))) {
-                            if (n < KP) {
-                                PV_L(n) = key;
-                                n++;
-                                if (n == KP) {
-                                    wi = 0;
-                                    for (int j = 1; j < KP; j++)
-                                        if (PV_L(j) > PV_L(wi)) wi = j;
-                                    lmax = PV_L(wi);
-                                    if (lmax < thr) {
-                                        thr = lmax;
-                                        thr_d = key_dist(lmax);
-                                    }
-                                }
-                            } else {
-                                PV_L(wi) = key;
-                                wi = 0;
-                                for (int j = 1; j < KP; j++)
-                                    if (PV_L(j) > PV_L(wi)) wi = j;
-                                lmax = PV_L(wi);
-                                if (lmax < thr) {
-                                    thr = lmax;
-                                    thr_d = key_dist(lmax);
-                                }
-                            }
+                        stage[i * NSLOT + slot] = d;
+                        cmask |= 1u << i;
+                    }
+                }
+                cmask &= bw[c];
+#pragma unroll 1
+                while (cmask) {
+                    const int i = __ffs(cmask) - 1;
+                    cmask &= cmask - 1;
+                    const float d = fmaxf(stage[i * NSLOT + slot], 0.f);
+                    const uint64_t row = rbase + c * 32 + i;
+                    const uint64_t key = make_key(d, (uint32_t)row);
+                    // <= : the seeded bound is itself a row key that this
+                    // pass must admit again (keys are unique)
+                    if (key > thr) continue;
+                    if (n < KP) {
+                        PV_L(n) = key;
+                        n++;
+                        if (n < KP) continue;
+                    } else {
+                        PV_L(wi) = key;
+                    }
+                    wi = 0;
+                    lmax = PV_L(0);
+                    for (int j = 1; j < KP; j++) {
+                        const uint64_t v = PV_L(j);
+                        if (v > lmax) {
+                            lmax = v;
+                            wi = j;
                         }
+                    }
+                    if (lmax < thr) {
+                        thr = lmax;
+                        thr_d = key_dist(lmax);
                     }
                 }
             }
             tc_fence_before();
             mbar_arrive(&tempty[acc]);
+            if (tr) a.trace[t * 4 + 3] = globaltimer();
             if (qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
+#pragma unroll
+            for (int j = 0; j < CPH; j++) {
+                xr[j] = nxr[j];
+                xs[j] = nxs[j];
+                bw[j] = nbw[j];
+            }
+            gt = ngt;
         }
         if (!ok) {
             s_abort = 1;
@@ -316,9 +366,11 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 }
                 PV_L(j + 1) = v;
             }
-            uint64_t *dst = a.part + ((uint64_t)qg * a.grow + rgrp) * KP;
+            // partial list (rgrp, half) of query qg; the merge sees grow*EPI lists
+            const uint64_t li = (uint64_t)qg * a.grow * EPI + (uint64_t)rgrp * EPI + half;
+            uint64_t *dst = a.part + li * KP;
             for (int i = 0; i < n; i++) dst[i] = PV_L(i);
-            a.part_cnt[(uint64_t)qg * a.grow + rgrp] = (uint32_t)n;
+            a.part_cnt[li] = (uint32_t)n;
         }
 #undef PV_L
     }
@@ -469,9 +521,24 @@ bool tc_supported(const FvGpuIndex *g) {
     return row_bytes <= 512;  // query tile <= 64 KB of shared memory
 }
 
-static size_t tc_smem(int kblocks, int NS, int KP) {
+static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
     return 1024 + (size_t)kblocks * TC_BOX + (size_t)NS * TC_KBS * TC_BOX +
-           (size_t)TC_BM * KP * 8 + (size_t)(2 * NS + 6) * 8;
+           (size_t)TC_BM * EPI * KP * 8 + (size_t)32 * TC_BM * EPI * 4 +
+           (size_t)(2 * NS + 6) * 8;
+}
+
+template <int EPI>
+static cudaError_t tc_launch(bool fp8, int grid, size_t smem, cudaStream_t st,
+                            const CUtensorMap &tmX, const CUtensorMap &tmQ, const TcArgs &a) {
+    const void *fn = fp8 ? (const void *)scan_tc_kernel<true, EPI>
+                         : (const void *)scan_tc_kernel<false, EPI>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (fp8)
+        scan_tc_kernel<true, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
+    else
+        scan_tc_kernel<false, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
+    return cudaGetLastError();
 }
 
 // Launches query prep, the tensor-core scan, the per-query merge and the
@@ -490,9 +557,17 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
         snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
         return -1;
     }
-    int NS = 4;
-    while (NS > 2 && tc_smem(kblocks, NS, KP) > 227 * 1024) NS--;
-    const size_t smem = tc_smem(kblocks, NS, KP);
+    // two epilogue warp groups (each row half of a tile) when the lists fit,
+    // with at least two pipeline stages; else one group
+    const size_t smem_cap = 227 * 1024;
+    int EPI = 2, NS = 4;
+    while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
+    if (tc_smem(kblocks, NS, KP, EPI) > smem_cap) {
+        EPI = 1;
+        NS = 4;
+        while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
+    }
+    const size_t smem = tc_smem(kblocks, NS, KP, EPI);
     const int qtiles = (nq + TC_BM - 1) / TC_BM;
     const int nqpad = qtiles * TC_BM;
     const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;
@@ -514,8 +589,9 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     const size_t cbytes = off_ctr + (size_t)nq + 256;
     PV_CUDA_OK(s.cand.ensure(cbytes), errbuf, errlen);
     PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
-    PV_CUDA_OK(s.part.ensure((size_t)nq * grow * KP * 8), errbuf, errlen);
-    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * grow * 4), errbuf, errlen);
+    const int nlists = grow * EPI;  // partial lists per query
+    PV_CUDA_OK(s.part.ensure((size_t)nq * nlists * KP * 8), errbuf, errlen);
+    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * nlists * 4), errbuf, errlen);
     unsigned char *c = s.cand.as<unsigned char>();
     int *d_err = (int *)(c + off_err);
     PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
@@ -553,18 +629,21 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     a.part_cnt = s.part_cnt.as<uint32_t>();
     a.err = d_err;
     a.timeout_ns = 2000000000ull;
-    PV_CUDA_OK(cudaFuncSetAttribute(fp8 ? (const void *)scan_tc_kernel<true>
-                                        : (const void *)scan_tc_kernel<false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-               errbuf, errlen);
+    a.trace = nullptr;
+    a.trace_tiles = 0;
+    static const bool tracing = getenv("PV_TC_TRACE") != nullptr;
+    static uint64_t *d_trace = nullptr;
+    if (tracing) {
+        if (!d_trace) cudaMalloc(&d_trace, 64 * 4 * 8);
+        if (d_trace) {
+            cudaMemsetAsync(d_trace, 0, 64 * 4 * 8, g->stream);
+            a.trace = d_trace;
+            a.trace_tiles = 64;
+        }
+    }
     auto run = [&](const TcArgs &args) {
-        if (fp8)
-            scan_tc_kernel<true><<<args.grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ,
-                                                                                     args);
-        else
-            scan_tc_kernel<false><<<args.grow * qtiles, TC_THREADS, smem, g->stream>>>(tmX, tmQ,
-                                                                                      args);
-        return cudaGetLastError();
+        return EPI == 2 ? tc_launch<2>(fp8, args.grow * qtiles, smem, g->stream, tmX, tmQ, args)
+                        : tc_launch<1>(fp8, args.grow * qtiles, smem, g->stream, tmX, tmQ, args);
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
@@ -580,8 +659,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
         PV_CUDA_OK(run(sa), errbuf, errlen);
         ScanPlan sp;
         sp.M = 1024;
-        sp.merge_smem = (size_t)sp.M * 8 + (size_t)grow * 8;
-        PV_CUDA_OK(launch_merge(a.part, a.part_cnt, grow, KP, sp, a.tau, d_qprog, popcnt,
+        sp.merge_smem = (size_t)sp.M * 8 + (size_t)nlists * 8;
+        PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, sp, a.tau, d_qprog, popcnt,
                                 g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
                                 a.tau),
                    errbuf, errlen);
@@ -592,8 +671,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     if (ev) cudaEventRecord(ev[2], g->stream);
     ScanPlan pl;
     pl.M = 1024;
-    pl.merge_smem = (size_t)pl.M * 8 + (size_t)grow * 8;
-    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, grow, KP, pl, a.tau, d_qprog, popcnt, g->count,
+    pl.merge_smem = (size_t)pl.M * 8 + (size_t)nlists * 8;
+    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, pl, a.tau, d_qprog, popcnt, g->count,
                             nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream),
                errbuf, errlen);
     rerank_kernel<<<nq, 128, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, KP, topb,
@@ -601,6 +680,16 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
     if (ev) cudaEventRecord(ev[3], g->stream);
     g->tc_err = d_err;
+    if (tracing && d_trace) {
+        uint64_t h[64 * 4];
+        cudaStreamSynchronize(g->stream);
+        cudaMemcpy(h, d_trace, sizeof(h), cudaMemcpyDeviceToHost);
+        const uint64_t t0 = h[0];
+        for (int t = 0; t < 64 && h[t * 4]; t++)
+            fprintf(stderr, "PVTRACE tile %d issue %.2f mma %.2f epi %.2f done %.2f us\n", t,
+                    (h[t * 4] - t0) / 1e3, (h[t * 4 + 1] - t0) / 1e3,
+                    (h[t * 4 + 2] - t0) / 1e3, (h[t * 4 + 3] - t0) / 1e3);
+    }
     return 0;
 }
 
