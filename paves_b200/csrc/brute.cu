@@ -88,7 +88,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
-    if (mode == 1 && tc_supported(g) && tc_superset(topb) > 0) {
+    if (mode == 1 && tc_supported(g) && tc_superset(g, topb) > 0) {
         if (launch_scan_tc(g, nq, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
                            errbuf, errlen))

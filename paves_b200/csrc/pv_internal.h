@@ -74,7 +74,7 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
                    uint8_t *truncated, char *errbuf, size_t errlen);
 
 // ---- tensor-core scan (scan_tc.cu)
-int tc_superset(uint32_t topb);
+int tc_superset(const FvGpuIndex *g, uint32_t topb);
 bool tc_supported(const FvGpuIndex *g);
 int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,

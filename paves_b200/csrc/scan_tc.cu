@@ -508,8 +508,13 @@ static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner,
     return r == CUDA_SUCCESS;
 }
 
-int tc_superset(uint32_t topb) {
-    int kp = 4 * (int)topb;
+// Candidates kept per query before the exact re-rank: 4k while the scan's
+// distances may be inexact; k itself when the upload certified that BF16
+// distances are exact (integer rows, |x| <= 256, all sums below 2^24), since
+// then the scan's top-k already is the exact top-k. 0 = topb too large.
+int tc_superset(const FvGpuIndex *g, uint32_t topb) {
+    const bool exact = g->int_exact && g->precision != FV_GPU_PREC_FP8;
+    int kp = exact ? (int)topb : 4 * (int)topb;
     if (kp > 64) kp = 64;
     if (kp < (int)topb) return 0;  // topb beyond the superset capacity
     return kp;
@@ -552,7 +557,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     const bool fp8 = g->precision == FV_GPU_PREC_FP8;
     const int esz = fp8 ? 1 : 2;
     const int kblocks = g->kpad * esz / TC_KB_BYTES;
-    const int KP = tc_superset(topb);
+    const int KP = tc_superset(g, topb);
     if (!KP || !tc_supported(g)) {
         snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
         return -1;
