@@ -270,6 +270,7 @@ def main():
 
     # per-kernel device times of the same steps (events between kernels)
     _, st = batch_run(b, args.steps, stages=True)
+    superset = int(_lib.lib().pv_last_superset(gi.handle))
     scan_ms = st[1] / args.steps
     hbm, bf16, peak_kind = load_peaks()
     # tensor-core scan: bf16 rows (128 dims = 256 B) + f32 norm, once per batch
@@ -326,8 +327,9 @@ def main():
             "data": "synthetic",
             "config": {"workload": "1M x 128 Gaussian-mixture rows (integer-valued), 64-query "
                                    "batches over six predicate classes 0.1%-95%, filtered "
-                                   "top-10; BF16 tensor-core scan + exact FP32 re-rank of 40",
+                                   "top-10; BF16 tensor-core scan + exact FP32 re-rank",
                        "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK,
+                       "rerank_candidates": superset,
                        "path": "bf16-scan", "l2_flush": "inputs larger than L2 (256 MB bf16 "
                                                         "rows, 512 MB f32 rows vs 126 MB)"},
             "recall_at_10_vs_exact": round(rec, 4),

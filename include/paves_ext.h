@@ -57,6 +57,11 @@ void pv_batch_free(PvBatch *b);
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 
+/* Candidates per query the last reduced-precision scan on g re-ranked in
+ * exact FP32 (4 x topb, or topb when its BF16 distances were certified
+ * exact: integer rows and queries with all sums below 2^24); 0 if none. */
+int pv_last_superset(const FvGpuIndex *g);
+
 /* Counters of the last fv_gpu_graph_batch call: per query [steps, visited,
  * predicate probes, results]; copies min(nq, last nq) rows, returns rows. */
 int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq);

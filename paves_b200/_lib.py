@@ -91,6 +91,7 @@ _EXT_SIGS = {
     "pv_batch_fetch": (C.c_int, [P, P, P, P, C.c_char_p, C.c_size_t]),
     "pv_batch_free": (None, [P]),
     "pv_last_kernel_ms": (C.c_float, [P]),
+    "pv_last_superset": (C.c_int, [P]),
     "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
 }
 PV_MODE_EXACT, PV_MODE_LOW = 0, 1

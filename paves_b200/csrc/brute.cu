@@ -48,6 +48,7 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
             memset(hq + (size_t)q * g->dpad + g->dim, 0, (size_t)(g->dpad - g->dim) * 4);
         }
     }
+    db.q_amax = pv_integral_amax(queries, (uint64_t)nq * g->dim);
     memcpy(h + db.off_qprog, pb.qprog.data(), (size_t)nq * 4);
     if (P) memcpy(h + db.off_progs, pb.progs.data(), (size_t)P * sizeof(PredProg));
     if (!pb.insns.empty())
@@ -88,8 +89,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
-    if (mode == 1 && tc_supported(g) && tc_superset(g, topb) > 0) {
-        if (launch_scan_tc(g, nq, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
+    if (mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0) {
+        if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
                            errbuf, errlen))
             return -1;

@@ -159,6 +159,8 @@ extern "C" void pv_batch_free(PvBatch *b) {
 
 extern "C" float pv_last_kernel_ms(const FvGpuIndex *g) { return g ? g->last_kernel_ms : 0.f; }
 
+extern "C" int pv_last_superset(const FvGpuIndex *g) { return g ? g->last_superset : 0; }
+
 extern "C" int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq) {
     if (!g || !out) return 0;
     int n = (int)(g->graph_stats.size() / 4);

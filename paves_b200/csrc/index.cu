@@ -119,21 +119,33 @@ static int pick_device(size_t need) {
     return best;
 }
 
-static bool rows_integral_exact(const float *v, uint64_t count, int dim) {
-    // the norm form ||x||^2 + ||q||^2 - 2 x.q is exact in fp32 for integer
-    // rows when every partial sum stays below 2^24 (bf16 holds integers up
-    // to 256 exactly)
+}  // namespace pv
+
+// Largest |value| of an array if every value is an integer of magnitude
+// <= 256 (exactly representable in bf16), else -1.
+float pv_integral_amax(const float *v, uint64_t n) {
     float amax = 0.f;
-    for (uint64_t i = 0; i < count * (uint64_t)dim; i++) {
-        float x = v[i];
-        if (x != floorf(x)) return false;
-        float a = fabsf(x);
+    for (uint64_t i = 0; i < n; i++) {
+        const float x = v[i];
+        if (x != floorf(x)) return -1.f;
+        const float a = fabsf(x);
         if (a > amax) amax = a;
-        if (amax > 256.f) return false;
+        if (amax > 256.f) return -1.f;
     }
-    double worst = 4.0 * (double)dim * amax * amax;  // ||x||^2+||q||^2+2|x.q|
+    return amax;
+}
+
+// True when bf16 tensor-core distances are exact for rows with integral
+// max row_amax and queries with integral max q_amax: the norm form's
+// largest intermediate, ||x||^2 + ||q||^2 <= dim * (row_amax^2 + q_amax^2),
+// and every partial dot product stay below 2^24.
+bool pv_bf16_exact(int dim, float row_amax, float q_amax) {
+    if (row_amax < 0.f || q_amax < 0.f) return false;
+    const double worst = (double)dim * ((double)row_amax * row_amax + (double)q_amax * q_amax);
     return worst < 16777216.0;
 }
+
+namespace pv {
 
 }  // namespace pv
 
@@ -267,7 +279,7 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         if (e != cudaSuccess) return bail("graph", e);
     }
 
-    g->int_exact = rows_integral_exact(vectors, count, dim);
+    g->row_amax = pv_integral_amax(vectors, count * (uint64_t)dim);
 
     if (precision != FV_GPU_PREC_FP32) {
         const bool f8 = precision == FV_GPU_PREC_FP8;

@@ -94,7 +94,7 @@ struct FvGpuIndex {
     void *d_vlow = nullptr;     // bf16 [count][kpad] or fp8 [count][kpad]
     float *d_vscale = nullptr;  // fp8 per-row scale
     float *d_norm = nullptr;    // ||x||^2 of the stored low-precision row
-    bool int_exact = false;     // rows integral, |x| <= 256, d*max^2 < 2^24
+    float row_amax = -1.f;      // max |x| if all rows are integers <= 256, else -1
 
     int sm_count = 0;
     cudaStream_t stream = nullptr;
@@ -104,6 +104,7 @@ struct FvGpuIndex {
     pv::ScanScratch scan;
     pv::GraphScratch graph;
     int *tc_err = nullptr;  // watchdog word of the last tensor-core scan (device)
+    int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels
     std::vector<uint32_t> graph_stats;  // last graph batch: [nq][4] counters
 };

@@ -3,6 +3,9 @@
 
 #include "index.h"
 
+float pv_integral_amax(const float *v, uint64_t n);
+bool pv_bf16_exact(int dim, float row_amax, float q_amax);
+
 namespace pv {
 
 // ---- predicates (pred.cpp, bitmap.cu)
@@ -59,6 +62,7 @@ struct DevBatch {
     int nq = 0, P = 0;
     size_t off_q = 0, off_qprog = 0, off_progs = 0, off_insns = 0, off_consts = 0, off_extra = 0;
     size_t bytes = 0;
+    float q_amax = -1.f;  // max |q| if all queries are integers <= 256, else -1
 };
 
 int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
@@ -74,9 +78,10 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
                    uint8_t *truncated, char *errbuf, size_t errlen);
 
 // ---- tensor-core scan (scan_tc.cu)
-int tc_superset(const FvGpuIndex *g, uint32_t topb);
+int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax);
 bool tc_supported(const FvGpuIndex *g);
-int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qprog,
+int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
+                   const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,

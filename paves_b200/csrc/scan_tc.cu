@@ -512,8 +512,9 @@ static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner,
 // distances may be inexact; k itself when the upload certified that BF16
 // distances are exact (integer rows, |x| <= 256, all sums below 2^24), since
 // then the scan's top-k already is the exact top-k. 0 = topb too large.
-int tc_superset(const FvGpuIndex *g, uint32_t topb) {
-    const bool exact = g->int_exact && g->precision != FV_GPU_PREC_FP8;
+int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax) {
+    const bool exact =
+        g->precision != FV_GPU_PREC_FP8 && pv_bf16_exact(g->dim, g->row_amax, q_amax);
     int kp = exact ? (int)topb : 4 * (int)topb;
     if (kp > 64) kp = 64;
     if (kp < (int)topb) return 0;  // topb beyond the superset capacity
@@ -549,7 +550,8 @@ static cudaError_t tc_launch(bool fp8, int grid, size_t smem, cudaStream_t st,
 // Launches query prep, the tensor-core scan, the per-query merge and the
 // exact re-rank. Inputs: f32 queries [nq][dpad] on the device, predicate
 // programs/bitmaps already built.
-int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qprog,
+int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
+                   const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
@@ -557,7 +559,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, const float *d_q, const int32_t *d_qpr
     const bool fp8 = g->precision == FV_GPU_PREC_FP8;
     const int esz = fp8 ? 1 : 2;
     const int kblocks = g->kpad * esz / TC_KB_BYTES;
-    const int KP = tc_superset(g, topb);
+    const int KP = tc_superset(g, topb, q_amax);
+    g->last_superset = KP;
     if (!KP || !tc_supported(g)) {
         snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
         return -1;
