@@ -97,13 +97,116 @@ bitmap_kernel(const double *__restrict__ cols, uint64_t nrows,
     if (threadIdx.x == 0 && s_cnt) atomicAdd(popcnt + p, (unsigned long long)s_cnt);
 }
 
+// All programs of a batch in one pass: a warp takes 4 consecutive 32-row
+// words and evaluates every program on them, 4 rows per lane in flight, so
+// a column's values are fetched from HBM once per batch and re-read from
+// L1 by the other programs. Programs and constants live in shared memory.
+constexpr int BM_MAX_INSNS = 512;
+constexpr int BM_MAX_PROGS = 1024;
+constexpr int BM_MAX_CONSTS = 512;
+
+__global__ void __launch_bounds__(256)
+bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
+                    const PredInsn *__restrict__ insns, int ninsns,
+                    const PredProg *__restrict__ progs, int P,
+                    const double *__restrict__ consts, int nconsts,
+                    uint32_t *__restrict__ bitmaps, uint64_t bm_words,
+                    unsigned long long *__restrict__ popcnt) {
+    __shared__ PredInsn s_ins[BM_MAX_INSNS];
+    __shared__ PredProg s_prog[BM_MAX_PROGS];
+    __shared__ double s_const[BM_MAX_CONSTS];
+    __shared__ unsigned int s_cnt[BM_MAX_PROGS];
+    for (int i = threadIdx.x; i < ninsns; i += blockDim.x) s_ins[i] = insns[i];
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        s_prog[i] = progs[i];
+        s_cnt[i] = 0;
+    }
+    for (int i = threadIdx.x; i < nconsts; i += blockDim.x) s_const[i] = consts[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t groups = (bm_words + 3) / 4;
+    const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t grp = gw; grp < groups; grp += nw) {
+        uint64_t row[4];
+        bool live[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            row[j] = (grp * 4 + j) * 32 + lane;
+            live[j] = row[j] < nrows;
+        }
+        for (int p = 0; p < P; p++) {
+            const PredProg pg = s_prog[p];
+            uint64_t st[4] = {0, 0, 0, 0};
+            for (int i = 0; i < pg.ninsn; i++) {
+                const PredInsn in = s_ins[pg.insn0 + i];
+                if (in.kind == FV_NODE_CMP || in.kind == FV_NODE_IN) {
+                    const double *c = cols + (uint64_t)in.col * nrows;
+                    double v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) v[j] = live[j] ? __ldg(c + row[j]) : 0.0;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        bool b;
+                        if (in.kind == FV_NODE_CMP) {
+                            b = cmp_op(v[j], in.op, in.value);
+                        } else {
+                            b = false;
+                            for (int k = 0; k < in.n; k++) b |= (v[j] == s_const[in.val0 + k]);
+                        }
+                        st[j] = (st[j] << 1) | (b ? 1u : 0u);
+                    }
+                } else if (in.kind == FV_NODE_AND || in.kind == FV_NODE_OR) {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        if (in.n == 0) {
+                            st[j] = (st[j] << 1) | (in.kind == FV_NODE_AND ? 1u : 0u);
+                        } else {
+                            const uint64_t b = st[j] & 3u;
+                            const bool r = in.kind == FV_NODE_AND ? b == 3u : b != 0u;
+                            st[j] = ((st[j] >> 2) << 1) | (r ? 1u : 0u);
+                        }
+                    }
+                } else {  // NOT
+#pragma unroll
+                    for (int j = 0; j < 4; j++) st[j] ^= 1u;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t word = __ballot_sync(0xffffffffu, live[j] && (st[j] & 1u));
+                const uint64_t w = grp * 4 + j;
+                if (lane == 0 && w < bm_words) {
+                    bitmaps[(uint64_t)p * bm_words + w] = word;
+                    if (word) atomicAdd(&s_cnt[p], (unsigned)__popc(word));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += blockDim.x)
+        if (s_cnt[p]) atomicAdd(popcnt + p, (unsigned long long)s_cnt[p]);
+}
+
 cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words,
-                           unsigned long long *popcnt, int sm_count, cudaStream_t st) {
+                           unsigned long long *popcnt, int sm_count, cudaStream_t st,
+                           int ninsns, int nconsts) {
     if (P <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(popcnt, 0, sizeof(unsigned long long) * P, st);
     if (e != cudaSuccess) return e;
+    if (ninsns <= BM_MAX_INSNS && P <= BM_MAX_PROGS && nconsts <= BM_MAX_CONSTS) {
+        const uint64_t groups = (bm_words + 3) / 4;
+        uint64_t blocks = (groups + 7) / 8;
+        const uint64_t cap = (uint64_t)sm_count * 4;
+        if (blocks > cap) blocks = cap;
+        if (blocks == 0) blocks = 1;
+        bitmap_multi_kernel<<<(unsigned)blocks, 256, 0, st>>>(cols, nrows, insns, ninsns, progs,
+                                                              P, consts, nconsts, bitmaps,
+                                                              bm_words, popcnt);
+        return cudaGetLastError();
+    }
     uint64_t blocks = (bm_words + 7) / 8;
     uint64_t cap = (uint64_t)sm_count * 8;
     if (blocks > cap) blocks = cap;

@@ -29,6 +29,8 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
     const int P = (int)pb.progs.size();
     db.nq = nq;
     db.P = P;
+    db.ninsns = (int)pb.insns.size();
+    db.nconsts = (int)pb.consts.size();
     db.off_q = 0;
     db.off_qprog = al256(qbytes);
     db.off_progs = db.off_qprog + al256((size_t)nq * 4);
@@ -84,7 +86,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
-                                  s.popcnt.as<unsigned long long>(), g->sm_count, g->stream),
+                                  s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
+                                  db.ninsns, db.nconsts),
                    errbuf, errlen);
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);

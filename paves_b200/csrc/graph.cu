@@ -427,7 +427,8 @@ int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *
                                   (const PredProg *)(d + db.off_progs),
                                   (const double *)(d + db.off_consts), P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
-                                  s.popcnt.as<unsigned long long>(), g->sm_count, g->stream),
+                                  s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
+                                  db.ninsns, db.nconsts),
                    errbuf, errlen);
     }
     PV_CUDA_OK(gs.visited.ensure((size_t)nq * bm_words * 4), errbuf, errlen);

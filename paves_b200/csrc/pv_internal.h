@@ -16,7 +16,7 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
 cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words, unsigned long long *popcnt,
-                           int sm_count, cudaStream_t st);
+                           int sm_count, cudaStream_t st, int ninsns, int nconsts);
 
 // ---- exact FP32 scan (scan_f32.cu)
 struct ScanF32Args {
@@ -59,7 +59,7 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
 struct DevBatch {
     Buf *stage_h = nullptr;
     Buf *stage_d = nullptr;
-    int nq = 0, P = 0;
+    int nq = 0, P = 0, ninsns = 0, nconsts = 0;
     size_t off_q = 0, off_qprog = 0, off_progs = 0, off_insns = 0, off_consts = 0, off_extra = 0;
     size_t bytes = 0;
     float q_amax = -1.f;  // max |q| if all queries are integers <= 256, else -1

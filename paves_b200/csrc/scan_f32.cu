@@ -185,17 +185,12 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
 
 // Reduces the per-CTA lists of one query to its final top-K (one CTA per
 // query). Only keys <= the grid-wide bound can be in the answer; lists are
-// ascending so each contributes a prefix. Prefixes are folded into the
-// running top-K in rounds that fit the shared buffer.
-__device__ __forceinline__ int prefix_le(const uint64_t *L, int c, uint64_t bound) {
-    int lo = 0, hi = c;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (L[mid] <= bound) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
+// ascending so each contributes a prefix. A warp measures a list's prefix
+// with one coalesced load + ballot per 32 entries, a warp scan turns the
+// lengths into offsets, and the gathered prefixes are sorted with a bitonic
+// network sized to their count. Prefixes that exceed the buffer are folded
+// into the running top-K in further rounds (rare: the bound keeps the
+// union near K).
 __global__ void __launch_bounds__(256)
 merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ part_cnt,
              int grow, int K, int M, const unsigned long long *__restrict__ tau,
@@ -207,47 +202,73 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
     uint64_t *buf = (uint64_t *)smem_raw;   // [M]
     int *s_c = (int *)(buf + M);            // [grow] prefix lengths
     int *s_off = s_c + grow;                // [grow] offsets within a round
-    __shared__ int s_gend;
+    __shared__ int s_gend, s_n;
     const int q = blockIdx.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nwarps = blockDim.x >> 5;
     const unsigned long long bound = tau[q];
     const uint64_t *lists = part + (uint64_t)q * grow * K;
     const uint32_t *cnts = part_cnt + (uint64_t)q * grow;
 
-    for (int i = tid; i < M; i += blockDim.x) buf[i] = KEY_MAX;
-    for (int g = tid; g < grow; g += blockDim.x) {
+    for (int g = warp; g < grow; g += nwarps) {
         int c = (int)cnts[g];
         if (c > K) c = K;
-        s_c[g] = prefix_le(lists + (uint64_t)g * K, c, bound);
+        const uint64_t *L = lists + (uint64_t)g * K;
+        int n = 0;
+        for (int j0 = 0; j0 < c; j0 += 32) {
+            const int j = j0 + lane;
+            const uint64_t key = j < c ? L[j] : KEY_MAX;
+            const uint32_t m = __ballot_sync(0xffffffffu, j < c && key <= bound);
+            n += __popc(m);
+            if (m != 0xffffffffu) break;
+        }
+        if (lane == 0) s_c[g] = n;
     }
     __syncthreads();
 
-    const int cap = M - K;
+    int nt = 0;  // valid keys in buf[0, K) carried between rounds
     int g = 0;
     while (g < grow) {
-        if (tid == 0) {
-            int n = 0, ge = g;
+        const int cap = M - nt;
+        if (warp == 0) {
+            // lists g.. in order while their prefixes fit (at least one list)
+            int base = 0, ge = g;
             while (ge < grow) {
-                const int c = s_c[ge];
-                if (n + c > cap && ge > g) break;
-                s_off[ge] = n;
-                n += c;
-                ge++;
+                const int i = ge + lane;
+                const int c = i < grow ? s_c[i] : 0;
+                int incl = c;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int excl = base + incl - c;
+                const bool fits = i < grow && (excl + c <= cap || i == g);
+                const uint32_t fm = __ballot_sync(0xffffffffu, fits);
+                const int nfit = __ffs(~fm) ? __ffs(~fm) - 1 : 32;  // leading run
+                if (lane < nfit) s_off[i] = nt + excl;
+                base += __shfl_sync(0xffffffffu, incl, nfit > 0 ? nfit - 1 : 0) * (nfit > 0);
+                ge += nfit;
+                if (nfit < 32) break;
             }
-            s_gend = ge;
+            if (lane == 0) {
+                s_gend = ge;
+                s_n = nt + base;
+            }
         }
         __syncthreads();
-        const int gend = s_gend;
-        const int warp = tid >> 5, lane = tid & 31;
-        for (int gg = g + warp; gg < gend; gg += blockDim.x / 32) {
+        const int gend = s_gend, n = s_n;
+        for (int gg = g + warp; gg < gend; gg += nwarps) {
             const uint64_t *L = lists + (uint64_t)gg * K;
-            const int c = s_c[gg], base = s_off[gg];
-            for (int i = lane; i < c; i += 32) buf[K + base + i] = L[i];
+            const int c = s_c[gg], off = s_off[gg];
+            for (int i = lane; i < c; i += 32) buf[off + i] = L[i];
         }
+        int n2 = 1;
+        while (n2 < n) n2 <<= 1;
+        for (int i = n + tid; i < n2; i += blockDim.x) buf[i] = KEY_MAX;
         __syncthreads();
-        for (int k = 2; k <= M; k <<= 1) {
+        for (int k = 2; k <= n2; k <<= 1) {
             for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < (M >> 1); i += blockDim.x) {
+                for (int i = tid; i < (n2 >> 1); i += blockDim.x) {
                     const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
                     const int hi = lo | j;
                     const uint64_t x = buf[lo], y = buf[hi];
@@ -260,10 +281,12 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
                 __syncthreads();
             }
         }
-        for (int i = K + tid; i < M; i += blockDim.x) buf[i] = KEY_MAX;
         __syncthreads();
+        nt = n < K ? n : K;
         g = gend;
     }
+    for (int i = nt + tid; i < K; i += blockDim.x) buf[i] = KEY_MAX;
+    __syncthreads();
     for (int i = tid; i < K; i += blockDim.x) {
         const uint64_t k = buf[i];
         if (k != KEY_MAX) {
