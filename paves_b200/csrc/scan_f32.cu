@@ -210,6 +210,52 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
     const uint64_t *lists = part + (uint64_t)q * grow * K;
     const uint32_t *cnts = part_cnt + (uint64_t)q * grow;
 
+    // fast path: one coalesced pass over all list slots; survivors (slot
+    // inside its list's count and key <= bound) are appended in any order,
+    // then sorted. Taken whenever they fit the buffer (the usual case).
+    for (int g = tid; g < grow; g += blockDim.x) {
+        const uint32_t c = cnts[g];
+        s_c[g] = c > (uint32_t)K ? K : (int)c;
+    }
+    if (tid == 0) s_n = 0;
+    __syncthreads();
+    {
+        const uint64_t total = (uint64_t)grow * K;
+        for (uint64_t i = tid; i < total; i += blockDim.x) {
+            const int g = (int)(i / K), j = (int)(i - (uint64_t)g * K);
+            if (j >= s_c[g]) continue;
+            const uint64_t key = lists[i];
+            if (key > bound) continue;
+            const int pos = atomicAdd(&s_n, 1);
+            if (pos < M) buf[pos] = key;
+        }
+    }
+    __syncthreads();
+    const int nfast = s_n;
+    if (nfast <= M) {
+        int n2 = 1;
+        while (n2 < nfast) n2 <<= 1;
+        for (int i = nfast + tid; i < n2; i += blockDim.x) buf[i] = KEY_MAX;
+        __syncthreads();
+        for (int k = 2; k <= n2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < (n2 >> 1); i += blockDim.x) {
+                    const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                    const int hi = lo | j;
+                    const uint64_t x = buf[lo], y = buf[hi];
+                    if ((x > y) == ((lo & k) == 0)) {
+                        buf[lo] = y;
+                        buf[hi] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        const int nt = nfast < K ? nfast : K;
+        for (int i = nt + tid; i < K; i += blockDim.x) buf[i] = KEY_MAX;
+        __syncthreads();
+    } else {
+    // general path: measure each list's prefix, then fold in rounds
     for (int g = warp; g < grow; g += nwarps) {
         int c = (int)cnts[g];
         if (c > K) c = K;
@@ -287,6 +333,7 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
     }
     for (int i = nt + tid; i < K; i += blockDim.x) buf[i] = KEY_MAX;
     __syncthreads();
+    }  // general path
     for (int i = tid; i < K; i += blockDim.x) {
         const uint64_t k = buf[i];
         if (k != KEY_MAX) {
@@ -379,7 +426,7 @@ bool plan_scan_f32(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPl
     pl.rows_per_cta = rpc;
     pl.grow = (int)((nrows + rpc - 1) / rpc);
     if (pl.grow < 1) pl.grow = 1;
-    pl.M = next_pow2(2 * K) < 1024 ? 1024 : next_pow2(2 * K);
+    pl.M = next_pow2(2 * K) < 4096 ? 4096 : next_pow2(2 * K);
     pl.merge_smem = (size_t)pl.M * 8 + (size_t)pl.grow * 8;
     return true;
 }

@@ -666,7 +666,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sa.tiles_per_cta = 1;
         PV_CUDA_OK(run(sa), errbuf, errlen);
         ScanPlan sp;
-        sp.M = 1024;
+        sp.M = 4096;
         sp.merge_smem = (size_t)sp.M * 8 + (size_t)nlists * 8;
         PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, sp, a.tau, d_qprog, popcnt,
                                 g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
@@ -678,7 +678,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
     ScanPlan pl;
-    pl.M = 1024;
+    pl.M = 4096;
     pl.merge_smem = (size_t)pl.M * 8 + (size_t)nlists * 8;
     PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, pl, a.tau, d_qprog, popcnt, g->count,
                             nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream),
