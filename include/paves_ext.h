@@ -54,6 +54,26 @@ int pv_batch_fetch(PvBatch *b, FvHit *out, uint32_t *out_cnt, uint8_t *truncated
 
 void pv_batch_free(PvBatch *b);
 
+/* Exact top-topb WITHOUT a predicate that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that must not
+ * allocate on the device while serving, because cudaMalloc synchronizes
+ * the whole device (a latency-bound serving loop cannot pay that per call)
+ * or because a framework that owns the device's memory forbids raw
+ * allocations. Scratch comes from one 2 MiB array linked into the library
+ * (held on every device that loads it until the process exits).
+ * d_queries (nq x dim f32), d_out (nq x topb FvHit) and d_cnt (nq u32) are
+ * DEVICE pointers on g's device, allocated by the caller however it may;
+ * results have the layout and order of fv_gpu_brute_batch (exact FP32).
+ * Limits: nq <= PV_NOALLOC_MAX_BATCH, topb <= PV_NOALLOC_MAX_TOPB, else -1
+ * with a message. The first call on a device looks up the array's device
+ * address, so make it before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race and must be serialized by the caller.
+ * Synchronous: returns after the results are in d_out / d_cnt. */
+#define PV_NOALLOC_MAX_BATCH 32
+#define PV_NOALLOC_MAX_TOPB 32
+int pv_brute_batch_noalloc(FvGpuIndex *g, int nq, const float *d_queries, uint32_t topb,
+                           FvHit *d_out, uint32_t *d_cnt, char *errbuf, size_t errlen);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 

@@ -90,6 +90,8 @@ _EXT_SIGS = {
     "pv_batch_run": (C.c_int, [P, C.c_int, P, P, C.c_char_p, C.c_size_t]),
     "pv_batch_fetch": (C.c_int, [P, P, P, P, C.c_char_p, C.c_size_t]),
     "pv_batch_free": (None, [P]),
+    "pv_brute_batch_noalloc": (C.c_int, [P, C.c_int, P, C.c_uint32, P, P, C.c_char_p,
+                                         C.c_size_t]),
     "pv_last_kernel_ms": (C.c_float, [P]),
     "pv_last_superset": (C.c_int, [P]),
     "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
