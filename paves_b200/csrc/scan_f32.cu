@@ -28,7 +28,9 @@ namespace pv {
 template <int QT>
 struct ScanShape {
     static constexpr int R = 32 / QT;           // rows per warp iteration
-    static constexpr int RPS = (QT >= 8) ? 128 : 256;  // rows per step
+    // rows per step (between block barriers); long steps for the small,
+    // bandwidth-bound tiles keep more loads in flight per warp
+    static constexpr int RPS = (QT >= 8) ? 128 : (QT >= 4 ? 256 : 1024);
     static constexpr int U = RPS / (8 * R);     // iterations per warp per step
     static constexpr int CB = 2 * RPS;
 };
@@ -102,11 +104,21 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
     const int my_q = lane % QT;
     const int my_qg = qt0 + my_q;
 
-    for (uint64_t sb = r0; sb < r1; sb += RPS) {
+    // The first step is one warp iteration (8 * R rows) so every query's
+    // threshold exists early; later steps are RPS rows.
+    int us = 1;
+    for (uint64_t sb = r0; sb < r1; sb += (uint64_t)8 * R * us, us = U) {
 #pragma unroll 1
-        for (int u = 0; u < U; u++) {
-            const uint64_t rb = sb + (uint64_t)(warp * U + u) * R;
+        for (int u = 0; u < us; u++) {
+            const uint64_t rb = sb + (uint64_t)(warp * us + u) * R;
             if (rb >= r1) break;
+            // predicate word of this lane's (row, query) pair, fetched with
+            // the rows so the filter never waits on a dependent load (the R
+            // rows of an iteration lie in one 32-row word)
+            const int my_pg = s_prog[my_q];
+            const uint32_t pword =
+                my_pg >= 0 ? __ldg(a.bitmaps + (uint64_t)my_pg * a.bm_words + (rb >> 5))
+                           : 0xFFFFFFFFu;
             float p[32];
 #pragma unroll
             for (int r = 0; r < R; r++) {
@@ -139,27 +151,25 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
             }
             const float dist = butterfly32(p, lane);
             const uint64_t row = rb + my_r;
-            if (row < r1 && my_qg < a.nq) {
+            if (row < r1 && my_qg < a.nq && ((pword >> (row & 31)) & 1u)) {
                 const uint64_t key = make_key(dist, (uint32_t)row);
                 if (key < t.tau[my_q]) {
-                    const int pg = s_prog[my_q];
-                    bool pass = true;
-                    if (pg >= 0)
-                        pass = (__ldg(a.bitmaps + (uint64_t)pg * a.bm_words + (row >> 5)) >>
-                                (row & 31)) & 1u;
-                    if (pass) {
-                        const int pos = atomicAdd(&t.nb[my_q], 1);
-                        t.region[(size_t)my_q * S + K + pos] = key;
-                    }
+                    const int pos = atomicAdd(&t.nb[my_q], 1);
+                    t.region[(size_t)my_q * S + K + pos] = key;
                 }
             }
         }
         __syncthreads();
-        const bool last = sb + RPS >= r1;
+        const bool last = sb + (uint64_t)8 * R * us >= r1;
         if (tid == 0) {
+            // flush when the next step could overflow the buffer, at the
+            // end, or as soon as a query without a full list has K keys
+            // (that sets its threshold)
             int n = 0;
             for (int qq = 0; qq < QT; qq++)
-                if (t.nb[qq] > 0 && (last || t.nb[qq] > CB - RPS)) t.flush_list[1 + n++] = qq;
+                if (t.nb[qq] > 0 && (last || t.nb[qq] > CB - RPS ||
+                                     (t.nt[qq] < K && t.nb[qq] >= K)))
+                    t.flush_list[1 + n++] = qq;
             t.flush_list[0] = n;
         }
         // pick up bounds published by other CTAs

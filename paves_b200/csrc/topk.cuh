@@ -31,9 +31,19 @@ __device__ __forceinline__ void topk_flush(TopkSmem &t, int S, int K, int CB,
                                            unsigned long long *__restrict__ g_tau) {
     const int nfl = t.flush_list[0];
     if (nfl == 0) return;
-    const int half = S >> 1;
+    // sort only the prefix that holds keys: [0, K) kept keys (KEY_MAX
+    // padded) and [K, K + nb) appended ones; everything past is KEY_MAX
+    int used = 0;
+    for (int f = 0; f < nfl; f++) {
+        const int nb = t.nb[t.flush_list[1 + f]];
+        if (nb > used) used = nb;
+    }
+    int n2 = 2;
+    while (n2 < K + used) n2 <<= 1;
+    if (n2 > S) n2 = S;
+    const int half = n2 >> 1;
     const int items = nfl * half;
-    for (int k = 2; k <= S; k <<= 1) {
+    for (int k = 2; k <= n2; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int it = threadIdx.x; it < items; it += blockDim.x) {
                 const int f = it / half;
@@ -52,9 +62,10 @@ __device__ __forceinline__ void topk_flush(TopkSmem &t, int S, int K, int CB,
         }
     }
     // cut back to K, clear the buffer area, update thresholds
-    for (int it = threadIdx.x; it < nfl * (S - K); it += blockDim.x) {
-        const int f = it / (S - K);
-        const int i = K + (it - f * (S - K));
+    const int tail = n2 > K ? n2 - K : 0;  // slots past the sorted prefix stay KEY_MAX
+    for (int it = threadIdx.x; it < nfl * tail; it += blockDim.x) {
+        const int f = it / tail;
+        const int i = K + (it - f * tail);
         t.region[(size_t)t.flush_list[1 + f] * S + i] = KEY_MAX;
     }
     if (threadIdx.x < nfl) {
