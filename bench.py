@@ -203,6 +203,31 @@ def fetch(b, nq, topb):
     return out["node"], out["dist"], cnt, tr
 
 
+KERNEL_CASES = {
+    # name: (batch, precision, mode, predicate kind index or None for rotation)
+    "exact_b1": (1, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, 5),
+    "exact_b64": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, None),
+    "bf16_b64": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, None),
+}
+
+
+def kernel_case(name, iters):
+    """One batch shape run `iters` times (device-resident inputs): the
+    small, self-contained program that ncu captures profile."""
+    nq, prec, mode, pk = KERNEL_CASES[name]
+    ds, preds, kinds = make_workload(nq=max(nq, 6))
+    if pk is not None:
+        preds = [preds[pk]] * nq
+    gi = GpuIndex(ds.vectors, ds.cols, precision=prec)
+    bp = pred.concat(preds[:nq], N_ROWS)
+    b = prepared_batch(gi, ds.queries[:nq], bp, TOPK, mode)
+    _, st = batch_run(b, iters, stages=True)
+    print(json.dumps({"case": name, "iters": iters,
+                      "stage_ms": [round(x / iters, 4) for x in st]}))
+    _lib.lib().pv_batch_free(b)
+    gi.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -210,7 +235,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES),
+                    help="run one batch shape --steps times and exit (for profilers)")
     args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args.kernel_case, max(1, args.steps))
+        return
     args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))
