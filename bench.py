@@ -370,7 +370,7 @@ def main():
                          "kernel": "scan_tc_kernel", "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
             "scan_gbs_batch1": round(scan_gbs_b1, 1),
-            "stage_ms": {"bitmap+prep": round(st[0] / args.steps, 4),
+            "stage_ms": {"bitmap+prep+seed": round(st[0] / args.steps, 4),
                          "scan": round(scan_ms, 4),
                          "merge+rerank": round(st[2] / args.steps, 4)},
             "clocks": clocks,

@@ -655,7 +655,6 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
-    if (ev) cudaEventRecord(ev[1], g->stream);
     // Seeding pass: one tile per CTA from an evenly strided sample; the
     // merged K'-th key of the sample bounds the K'-th key of the whole
     // scan, so the main pass admits only rows that can still matter.
@@ -673,6 +672,9 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                                 a.tau),
                    errbuf, errlen);
     }
+    // stage boundary: everything before the main pass (bitmaps, query prep,
+    // seeding) is stage 0, the main pass alone is stage 1
+    if (ev) cudaEventRecord(ev[1], g->stream);
     a.tile0_mul = tpc;
     a.tile_step = 1;
     PV_CUDA_OK(run(a), errbuf, errlen);
