@@ -44,6 +44,16 @@ METRIC = "filtered top-10 QPS, 1M x 128 L2"
 N_ROWS, DIM, BATCH, TOPK = 1_000_000, 128, 64, 10
 
 
+def load_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return int(json.load(f)[kernel]["bytes_per_launch"])
+    except Exception:
+        return None
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -366,7 +376,8 @@ def main():
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
                           "path": "exact FP32 scan", "scan_ms": round(plain_scan_ms, 4)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
-                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                         "traffic": load_traffic("scan_tc_kernel"),
                          "kernel": "scan_tc_kernel", "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
             "scan_gbs_batch1": round(scan_gbs_b1, 1),

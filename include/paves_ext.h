@@ -74,6 +74,29 @@ void pv_batch_free(PvBatch *b);
 int pv_brute_batch_noalloc(FvGpuIndex *g, int nq, const float *d_queries, uint32_t topb,
                            FvHit *d_out, uint32_t *d_cnt, char *errbuf, size_t errlen);
 
+/* ---- HNSW construction (host, multi-threaded) ----
+ * Builds the graph sections of a PAVES index file for count x dim rows
+ * (kept borrowed during the call): M = upper-level degree, 2M at level 0,
+ * ef_construction beam width, threads <= 0 = all cores. Same construction
+ * as the engine's builder (engine_api.h:45 fv_builder_finish), so files
+ * written from it open in the engine. NULL + errbuf on bad parameters. */
+typedef struct PvHnsw PvHnsw;
+PvHnsw *pv_hnsw_build(const float *vectors, uint64_t count, int dim, int M,
+                      int ef_construction, int threads, char *errbuf, size_t errlen);
+void pv_hnsw_free(PvHnsw *h);
+/* M, top level, entry node and the number of u32 upper-level slots. */
+int pv_hnsw_info(const PvHnsw *h, uint32_t *M, int *max_level, uint64_t *entry,
+                 uint64_t *upper_len);
+/* Copies the sections: l0 [count][2M+1], levels [count], upper_offs
+ * [count+1], upper [upper_len] (any pointer may be NULL). */
+int pv_hnsw_export(const PvHnsw *h, uint32_t *l0, uint8_t *levels, uint64_t *upper_offs,
+                   uint32_t *upper);
+/* Level-0 entry point per query by greedy descent through the upper levels
+ * (engine_api.h:199 fv_index_graph_entry), parallel over queries. */
+int pv_hnsw_entries(const float *vectors, int dim, const uint64_t *upper_offs,
+                    const uint32_t *upper, uint32_t M, int max_level, uint64_t entry,
+                    const float *queries, int nq, uint32_t *out, int threads);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 

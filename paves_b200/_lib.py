@@ -92,6 +92,13 @@ _EXT_SIGS = {
     "pv_batch_free": (None, [P]),
     "pv_brute_batch_noalloc": (C.c_int, [P, C.c_int, P, C.c_uint32, P, P, C.c_char_p,
                                          C.c_size_t]),
+    "pv_hnsw_build": (P, [P, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p,
+                          C.c_size_t]),
+    "pv_hnsw_free": (None, [P]),
+    "pv_hnsw_info": (C.c_int, [P, P, P, P, P]),
+    "pv_hnsw_export": (C.c_int, [P, P, P, P, P]),
+    "pv_hnsw_entries": (C.c_int, [P, C.c_int, P, P, C.c_uint32, C.c_int, C.c_uint64, P, C.c_int,
+                                  P, C.c_int]),
     "pv_last_kernel_ms": (C.c_float, [P]),
     "pv_last_superset": (C.c_int, [P]),
     "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
