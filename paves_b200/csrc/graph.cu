@@ -30,7 +30,7 @@ namespace pv {
 
 constexpr int G_THREADS = 256;
 constexpr int G_HC = 4096;   // visited hash slots (u32)
-constexpr int G_FC = 1024;   // frontier capacity
+constexpr int G_FC = 8192;   // frontier capacity (selective filters grow it)
 constexpr int G_RC = 512;    // result capacity (FV_GPU_MAX_EF)
 constexpr int G_NB = 512;    // new entries per step (W * deg_cap <= G_NB)
 constexpr uint32_t G_EMPTY = 0xFFFFFFFFu;
