@@ -97,6 +97,91 @@ int pv_hnsw_entries(const float *vectors, int dim, const uint64_t *upper_offs,
                     const uint32_t *upper, uint32_t M, int max_level, uint64_t entry,
                     const float *queries, int nq, uint32_t *out, int threads);
 
+/* ---- GPU worker micro-batch loop (request slots + one worker thread) ----
+ * Replaces the PostgreSQL background worker and shared-memory arbiter of
+ * the reference (arbiter.h:106-162 FvArbSlot/FvArbiter, arbiter.h:253
+ * paves_arbiter_submit, worker.c:149-598) for a process that serves from
+ * several threads. Backends call pv_arbiter_submit from any thread; one
+ * worker thread gathers SUBMITTED slots for up to wait_us (leaving after
+ * idle_us without arrivals), groups them by (relid, strategy), runs one
+ * batch per group through the executor (fv_gpu_brute_batch /
+ * fv_gpu_graph_batch unless replaced) and answers each slot. */
+#define PV_ARB_MAX_DIM 2000
+#define PV_ARB_MAX_NODES 48
+#define PV_ARB_MAX_CHILDREN 96
+#define PV_ARB_MAX_INVALS 128
+#define PV_ARB_MAX_SPANS 128
+#define PV_ARB_MAX_RESULTS 1024
+#define PV_STRAT_GPU_BRUTE 3 /* paves.h:48 FV_STRAT_GPU_BRUTE */
+#define PV_STRAT_GPU_HNSW 4  /* paves.h:49 FV_STRAT_GPU_HNSW */
+
+typedef struct PvArbiter PvArbiter;
+
+/* One batch as the worker hands it to an executor: the arguments of
+ * fv_gpu_brute_batch (strategy PV_STRAT_GPU_BRUTE) or fv_gpu_graph_batch
+ * (PV_STRAT_GPU_HNSW, qd[i].entry set, want = ef). flags = truncated /
+ * exhausted per query. Returns >= 0 or -1. */
+typedef struct PvArbBatch {
+    FvGpuIndex *g;
+    int strategy, nq, dim;
+    const float *queries;
+    const FvGpuQueryDesc *qd;
+    const uint8_t *dedup;
+    const FvGpuPredNode *nodes;
+    int nnodes;
+    const int32_t *children;
+    int nchildren;
+    const double *invals;
+    int ninvals;
+    const FvGpuSpan *spans;
+    int nspans;
+    const uint64_t *spanoff;
+    int nspanoff;
+    uint32_t want;
+    uint64_t max_visited;
+    FvHit *out;
+    uint32_t *out_cnt;
+    uint8_t *flags;
+} PvArbBatch;
+typedef int (*pv_arb_exec_fn)(void *ctx, const PvArbBatch *b);
+
+/* nslots request slots (512 in the reference), batches of at most
+ * batch_max requests; starts the worker thread. NULL on bad arguments. */
+PvArbiter *pv_arbiter_create(int nslots, int batch_max, int wait_us, int idle_us);
+/* Registers an index under relid: ino identifies the file (requests with
+ * another ino are answered ERROR), tids[count] maps rows to heap tids (NULL
+ * = row numbers), vectors/upper_offs/upper/M/max_level/entry give the upper
+ * levels for the graph entry descent (upper NULL = start at entry). All
+ * borrowed until pv_arbiter_destroy. 0 or -1. */
+int pv_arbiter_attach(PvArbiter *a, uint32_t relid, uint64_t ino, FvGpuIndex *g,
+                      const uint64_t *tids, uint64_t count, int dim, const float *vectors,
+                      const uint64_t *upper_offs, const uint32_t *upper, uint32_t M,
+                      int max_level, uint64_t entry);
+/* Replaces the executor (NULL restores the GPU batch calls). */
+void pv_arbiter_set_executor(PvArbiter *a, pv_arb_exec_fn fn, void *ctx);
+/* One request; blocks until answered. Returns 1 with out[*ncnt] (node =
+ * tid) and *more filled, 0 when no slot/worker is available, a capacity is
+ * exceeded or the worker did not answer within timeout_ms (<= 0: 10 s) and
+ * the slot was reclaimed (the caller keeps the query), -1 when the worker
+ * answered ERROR (same meaning as arbiter.h:253 paves_arbiter_submit). */
+int pv_arbiter_submit(PvArbiter *a, uint32_t relid, uint64_t ino, int strategy, int dim,
+                      const float *query, const FvGpuPredNode *nodes, int nnodes,
+                      const int32_t *children, int nchildren, const double *invals,
+                      int ninvals, const FvGpuSpan *spans, int nspans, int need_eval,
+                      int dedup, uint32_t want, uint64_t max_visited, int sel_permille,
+                      FvHit *out, uint32_t *ncnt, uint8_t *more, int timeout_ms);
+/* Batches run, requests served, requests waiting, worker alive (0/1). */
+int pv_arbiter_stats(PvArbiter *a, uint64_t *batches, uint64_t *requests, uint32_t *inflight,
+                     int *worker_ready);
+/* Service-time EWMAs of (relid, strategy) in us (arbiter.h:80-97):
+ * q_us[5] per selectivity bucket, whole batch, batch size x16. -1 if none. */
+int pv_arbiter_feedback(PvArbiter *a, uint32_t relid, int strategy, uint32_t *q_us,
+                        uint32_t *batch_us, uint32_t *batch_n16);
+/* Failure injection on the host: the worker exits after its current batch
+ * without answering it (a crashed worker); waiting backends reclaim. */
+void pv_arbiter_kill_worker(PvArbiter *a);
+void pv_arbiter_destroy(PvArbiter *a);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 

@@ -134,3 +134,31 @@ def ptr(a):
     if a is None:
         return None
     return a.ctypes.data if a.size else None
+
+
+class PvArbBatch(C.Structure):
+    _fields_ = [("g", P), ("strategy", C.c_int), ("nq", C.c_int), ("dim", C.c_int),
+                ("queries", P), ("qd", P), ("dedup", P), ("nodes", P), ("nnodes", C.c_int),
+                ("children", P), ("nchildren", C.c_int), ("invals", P), ("ninvals", C.c_int),
+                ("spans", P), ("nspans", C.c_int), ("spanoff", P), ("nspanoff", C.c_int),
+                ("want", C.c_uint32), ("max_visited", C.c_uint64), ("out", P), ("out_cnt", P),
+                ("flags", P)]
+
+
+PV_ARB_EXEC_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(PvArbBatch))
+PV_STRAT_GPU_BRUTE, PV_STRAT_GPU_HNSW = 3, 4
+PV_ARB_MAX_DIM, PV_ARB_MAX_NODES, PV_ARB_MAX_RESULTS = 2000, 48, 1024
+
+_EXT_SIGS.update({
+    "pv_arbiter_create": (P, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "pv_arbiter_attach": (C.c_int, [P, C.c_uint32, C.c_uint64, P, P, C.c_uint64, C.c_int, P, P,
+                                    P, C.c_uint32, C.c_int, C.c_uint64]),
+    "pv_arbiter_set_executor": (None, [P, PV_ARB_EXEC_FN, P]),
+    "pv_arbiter_submit": (C.c_int, [P, C.c_uint32, C.c_uint64, C.c_int, C.c_int, P, P, C.c_int,
+                                    P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, C.c_int,
+                                    C.c_uint32, C.c_uint64, C.c_int, P, P, P, C.c_int]),
+    "pv_arbiter_stats": (C.c_int, [P, P, P, P, P]),
+    "pv_arbiter_feedback": (C.c_int, [P, C.c_uint32, C.c_int, P, P, P]),
+    "pv_arbiter_kill_worker": (None, [P]),
+    "pv_arbiter_destroy": (None, [P]),
+})
