@@ -182,6 +182,76 @@ int pv_arbiter_feedback(PvArbiter *a, uint32_t relid, int strategy, uint32_t *q_
 void pv_arbiter_kill_worker(PvArbiter *a);
 void pv_arbiter_destroy(PvArbiter *a);
 
+/* ---- learned router (no counterpart in the reference) ----
+ * A 12 -> 64 -> 64 -> 5 MLP (ReLU; bf16 weights, fp32 accumulation) that
+ * predicts per query one action: 0 = exact/low-precision scan, 1..4 =
+ * graph search at ef 32, 64, 128, 256. It stands beside the reference's
+ * plain rule (planner.c:185-346 cost model, exec.c:415-424 beam width),
+ * which stays the fallback. Features per query (12 floats):
+ *   [0] log10(selectivity) from the query's predicate bitmap popcount
+ *   [1] |q|   [2..9] distances to the 8 nearest centroids, ascending
+ *   [10] log2(k)   [11] predicate root kind (0 none, 1 CMP, 2 IN, 3 AND,
+ *   4 OR, 5 NOT).
+ * Parameters (PV_MLP_NPARAMS fp32, the optimizer's master copy): W1
+ * [12][64], b1 [64], W2 [64][64], b2 [64], W3 [64][5], b3 [5], row-major
+ * with the input index first. */
+#define PV_MLP_IN 12
+#define PV_MLP_HIDDEN 64
+#define PV_MLP_OUT 5
+#define PV_MLP_NPARAMS (12 * 64 + 64 + 64 * 64 + 64 + 64 * 5 + 5)
+typedef struct PvRouter PvRouter;
+/* centroids [ncent][dim] (8 <= ncent <= 65536) are copied to the device. */
+PvRouter *pv_router_create(int device, const float *centroids, int ncent, int dim,
+                           char *errbuf, size_t errlen);
+void pv_router_free(PvRouter *r);
+/* Sets the master weights and the feature standardization (x - mean) / std;
+ * resets the optimizer state. */
+int pv_router_set_params(PvRouter *r, const float *params, const float *feat_mean,
+                         const float *feat_std, char *errbuf, size_t errlen);
+int pv_router_get_params(PvRouter *r, float *params, float *feat_mean, float *feat_std);
+/* Features of a batch on g's device (predicate arrays as fv_gpu_brute_batch,
+ * k[nq] per query) -> feats [nq][12]. */
+int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const float *queries,
+                       const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
+                       const int32_t *children, int nchildren, const double *invals,
+                       int ninvals, const uint32_t *k, float *feats, char *errbuf,
+                       size_t errlen);
+/* Logits [n][5] of feats [n][12] (raw features; standardized inside). */
+int pv_router_forward(PvRouter *r, int n, const float *feats, float *logits, char *errbuf,
+                      size_t errlen);
+/* Gradient of the sample-weighted mean cross-entropy over the n samples
+ * with respect to the parameters (through the bf16 forward), and the loss.
+ * sample_w may be NULL (all 1). */
+int pv_router_grad(PvRouter *r, int n, const float *feats, const int32_t *labels,
+                   const float *sample_w, float *grad, float *loss, char *errbuf,
+                   size_t errlen);
+/* Adam (beta 0.9/0.999, eps 1e-8) on shuffled minibatches of `batch`
+ * samples, floor(n / batch) steps per epoch, each step one CUDA graph
+ * launch; epoch_loss[epochs] receives the mean batch loss per epoch. */
+int pv_router_train(PvRouter *r, int n, const float *feats, const int32_t *labels,
+                    const float *sample_w, int epochs, int batch, float lr, uint64_t seed,
+                    float *epoch_loss, char *errbuf, size_t errlen);
+
+/* Learned-routed filtered top-k batch (no reference counterpart): builds
+ * the batch's predicate bitmaps, computes the router's features and MLP
+ * action per query on the device, then runs the graph search for the whole
+ * batch (per-query ef) when every query was routed to the graph, else the
+ * scan of the index's precision for the whole batch (a scan costs the same
+ * for one query as for a query tile, and its results are exact, so a batch
+ * with any scan-routed query scans). plan (optional, replaces the router,
+ * r may then be NULL): per query 0 = scan or the beam width to use. k[nq]
+ * <= topb; out has stride topb and holds min(k, found) hits per query.
+ * qd[i].entry must hold the level-0 entry point when the index has a
+ * graph. decided[nq] (optional) receives each query's beam width (0 =
+ * scan), *executed 1 for the graph, 0 for the scan; stage_ms[3] the device
+ * time of bitmaps, routing (incl. reading the decision back) and search. */
+int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *queries,
+                    const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
+                    const int32_t *children, int nchildren, const double *invals, int ninvals,
+                    const uint32_t *k, uint32_t topb, const uint16_t *plan, float margin,
+                    FvHit *out, uint32_t *out_cnt, uint16_t *decided, int *executed,
+                    float *stage_ms, char *errbuf, size_t errlen);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 

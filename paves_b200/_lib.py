@@ -162,3 +162,21 @@ _EXT_SIGS.update({
     "pv_arbiter_kill_worker": (None, [P]),
     "pv_arbiter_destroy": (None, [P]),
 })
+
+PV_MLP_IN, PV_MLP_HIDDEN, PV_MLP_OUT = 12, 64, 5
+PV_MLP_NPARAMS = 12 * 64 + 64 + 64 * 64 + 64 + 64 * 5 + 5
+_EXT_SIGS.update({
+    "pv_router_create": (P, [C.c_int, P, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
+    "pv_router_free": (None, [P]),
+    "pv_router_set_params": (C.c_int, [P, P, P, P, C.c_char_p, C.c_size_t]),
+    "pv_router_get_params": (C.c_int, [P, P, P, P]),
+    "pv_router_features": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int, P,
+                                     P, C.c_char_p, C.c_size_t]),
+    "pv_router_forward": (C.c_int, [P, C.c_int, P, P, C.c_char_p, C.c_size_t]),
+    "pv_router_grad": (C.c_int, [P, C.c_int, P, P, P, P, P, C.c_char_p, C.c_size_t]),
+    "pv_router_train": (C.c_int, [P, C.c_int, P, P, P, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                  P, C.c_char_p, C.c_size_t]),
+})
+_EXT_SIGS["pv_routed_batch"] = (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int,
+                                          P, C.c_uint32, P, C.c_float, P, P, P, P, P, C.c_char_p,
+                                          C.c_size_t])

@@ -69,7 +69,7 @@ int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen) {
 // Device-side work of one batch: inputs already resident in db.stage_d.
 int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
                  uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
-                 cudaEvent_t *ev) {
+                 cudaEvent_t *ev, bool bitmaps_ready) {
     const int nq = db.nq, P = db.P;
     char *d = db.stage_d->as<char>();
     const float *d_q = (const float *)(d + db.off_q);
@@ -81,7 +81,9 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     ScanScratch &s = g->scan;
 
     if (ev) cudaEventRecord(ev[0], g->stream);
-    if (P > 0) {
+    if (bitmaps_ready) {
+        // the caller launched the bitmaps of this batch
+    } else if (P > 0) {
         PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
         PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,

@@ -12,12 +12,15 @@
 //  * visited set: open-addressing hash of node ids; past half load it
 //    spills into a per-query global bitmap that the kernel zeroes itself,
 //    so there is no per-batch O(nq * N) memset;
-//  * frontier and results: ascending key arrays (dist bits << 32 | node)
-//    kept sorted by merge-path merges of each step's sorted new entries;
-//  * the step expands the best W frontier nodes at once (W adapts to the
-//    frontier size), gathers their neighbours from the fixed-width device
-//    adjacency, and computes distances with 8 lanes per node (16-byte
-//    loads), so 32 rows are in flight per CTA;
+//  * frontier and results: ascending key arrays (dist bits << 32 | node);
+//    each step's new keys are placed by rank (a count among the new keys
+//    plus a binary search in the old list), so no step sorts, and frontier
+//    entries beyond the worst of a full result list are dropped;
+//  * the step expands the best W frontier nodes at once (up to 16, fewer
+//    only when the rest cannot beat the worst result), gathers their
+//    neighbours from the fixed-width device adjacency, and computes
+//    distances with 4 lanes per node (16-byte loads), so 128 rows are in
+//    flight per CTA;
 //  * the predicate is a bit of the batch bitmap, read only for candidates
 //    that beat the current worst result.
 #include <string.h>
@@ -42,12 +45,14 @@ struct GraphArgs {
     const uint32_t *__restrict__ adj;
     const uint16_t *__restrict__ deg;
     int deg_cap;
+    int dc_shift;  // log2(deg_cap) when a power of two, else -1
     const float *__restrict__ queries;  // [nq][dpad]
     const uint32_t *__restrict__ entries;
     const int32_t *__restrict__ qprog;
     const uint32_t *__restrict__ bitmaps;
     uint64_t bm_words;
     int ef;
+    const uint16_t *__restrict__ efq;  // optional per-query ef (<= ef)
     uint64_t max_visited;
     int wmax;
     uint32_t *visited_bits;  // [nq][bm_words], zeroed by the kernel on spill
@@ -66,58 +71,81 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
     return x;
 }
 
-// Block-wide merge of ascending A[0,na) and B[0,nb) into C[0,min(na+nb,cap)).
-__device__ __forceinline__ void merge_path(const uint64_t *A, int na, const uint64_t *B, int nb,
-                                           uint64_t *C, int cap) {
-    const int total = min(na + nb, cap);
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        int lo = max(0, i - nb), hi = min(i, na);
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (A[mid] < B[i - mid - 1]) lo = mid + 1; else hi = mid;
-        }
-        const int a = lo, b = i - lo;
-        C[i] = (a < na && (b >= nb || A[a] < B[b])) ? A[a] : B[b];
-    }
-}
+// A result/frontier key carries the node's predicate bit in bit 31 of the
+// row half (rows < 2^31 are required), so one sort orders the keys and
+// keeps each key's bit. Among passing keys the order is (dist, node).
+constexpr uint32_t G_PASS = 0x80000000u;
+__device__ __forceinline__ uint32_t grow_of(uint64_t k) { return (uint32_t)k & ~G_PASS; }
 
-// Block-wide ascending bitonic sort of buf[0, n2), n2 a power of two.
-__device__ __forceinline__ void bitonic_block(uint64_t *buf, int n2) {
+// Ascending bitonic sort of buf[0, n2) (n2 a power of two, 64 <= n2 <=
+// 2 * G_THREADS). Only the n2 / 2 threads that own elements take part:
+// thread t holds elements 2t and 2t + 1 in registers; partners at most 32
+// elements away are exchanged by warp shuffles, farther ones through buf /
+// alt alternately, with a named barrier over the participating warps. The
+// caller synchronizes the block afterwards.
+__device__ __forceinline__ void block_sort_pairs(uint64_t *buf, uint64_t *alt, int n2) {
+    const int t = threadIdx.x;
+    const int nact = n2 >> 1;  // a multiple of 32
+    if (t >= nact) return;
+    const int i0 = 2 * t, i1 = i0 + 1;
+    uint64_t e0 = buf[i0], e1 = buf[i1];
+    int which = 0;
     for (int k = 2; k <= n2; k <<= 1) {
+        const bool asc = (i0 & k) == 0;  // same for i1: k >= 2
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
-                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-                const int hi = lo | j;
-                const uint64_t x = buf[lo], y = buf[hi];
-                if ((x > y) == ((lo & k) == 0)) {
-                    buf[lo] = y;
-                    buf[hi] = x;
-                }
+            if (j == 1) {
+                const bool lt = e0 < e1;
+                const uint64_t lo = lt ? e0 : e1, hi = lt ? e1 : e0;
+                e0 = asc ? lo : hi;
+                e1 = asc ? hi : lo;
+                continue;
             }
-            __syncthreads();
+            uint64_t o0, o1;
+            if (j <= 32) {
+                o0 = __shfl_xor_sync(0xffffffffu, e0, j >> 1);
+                o1 = __shfl_xor_sync(0xffffffffu, e1, j >> 1);
+            } else {
+                uint64_t *bb = which ? alt : buf;
+                which ^= 1;
+                bb[i0] = e0;
+                bb[i1] = e1;
+                asm volatile("bar.sync 1, %0;" ::"r"(nact) : "memory");
+                o0 = bb[i0 ^ j];
+                o1 = bb[i1 ^ j];
+            }
+            const bool keep_min = ((i0 & j) == 0) == asc;  // same for i1: j >= 2
+            e0 = ((e0 < o0) == keep_min) ? e0 : o0;
+            e1 = ((e1 < o1) == keep_min) ? e1 : o1;
         }
     }
+    asm volatile("bar.sync 1, %0;" ::"r"(nact) : "memory");
+    buf[i0] = e0;
+    buf[i1] = e1;
 }
 
 __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *const fr0 = (uint64_t *)smem_raw;  // [2][G_FC] frontier ping-pong
     uint64_t *const rs0 = fr0 + 2 * G_FC;        // [2][G_RC] results ping-pong
-    uint64_t *nfk = rs0 + 2 * G_RC;                // [G_NB] new frontier keys
-    uint64_t *nrk = nfk + G_NB;                   // [G_NB] new result keys
-    uint32_t *hash = (uint32_t *)(nrk + G_NB);    // [G_HC]
+    uint64_t *nfk = rs0 + 2 * G_RC;                // [G_NB] new keys (step order)
+    uint64_t *salt = nfk + G_NB;                  // [G_NB] sort exchange buffer
+    uint32_t *hash = (uint32_t *)(salt + G_NB);   // [G_HC]
     uint32_t *nid = hash + G_HC;                  // [G_NB] gathered neighbours
-    float *sq = (float *)(nid + G_NB);            // [dpad] query
+    int *rpos = (int *)(nid + G_NB);              // [G_NB] new results' places
+    int *fpos = rpos + G_NB;                      // [G_NB] new frontier keys' places
+    float *sq = (float *)(fpos + G_NB);           // [dpad] query
 
-    __shared__ int s_nf, s_nr, s_head, s_cur_f, s_cur_r, s_nsel, s_nnew, s_nfk, s_nrk;
-    __shared__ int s_stop, s_exh, s_spilled, s_hcount;
+    __shared__ int s_nf, s_nr, s_head, s_cur_f, s_cur_r, s_nsel, s_nnew, s_nfk;
+    __shared__ int s_wpass[G_THREADS / 32];
+    __shared__ int s_stop, s_exh, s_spilled, s_hcount, s_dropped;
     __shared__ uint32_t s_sel[32];
     __shared__ unsigned long long s_visited;
     __shared__ unsigned int s_probes, s_steps;
 
     const int q = blockIdx.x;
     const int tid = threadIdx.x;
-    const int ef = a.ef;
+    // per-query beam width (never above the batch's, which is the output stride)
+    const int ef = a.efq ? max(1, min((int)a.efq[q], a.ef)) : a.ef;
     const int pg = a.qprog[q];
     const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
     uint32_t *vb = a.visited_bits + (uint64_t)q * a.bm_words;
@@ -127,7 +155,7 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
     for (int i = tid; i < G_HC; i += blockDim.x) hash[i] = G_EMPTY;
     if (tid == 0) {
         s_nf = 0; s_nr = 0; s_head = 0; s_cur_f = 0; s_cur_r = 0;
-        s_stop = 0; s_exh = 0; s_spilled = 0; s_hcount = 0;
+        s_stop = 0; s_exh = 0; s_spilled = 0; s_hcount = 0; s_dropped = 0;
         s_visited = 0; s_probes = 0; s_steps = 0;
     }
     __syncthreads();
@@ -152,10 +180,10 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
                 hash[hash_u32(ep) & (G_HC - 1)] = ep;
                 s_hcount = 1;
                 s_visited = 1;
-                const uint64_t key = make_key(acc, ep);
+                const bool pass = !bm || ((bm[ep >> 5] >> (ep & 31)) & 1u);
+                const uint64_t key = make_key(acc, ep | (pass ? G_PASS : 0u));
                 fr0[0] = key;
                 s_nf = 1;
-                const bool pass = !bm || ((bm[ep >> 5] >> (ep & 31)) & 1u);
                 if (pass) {
                     rs0[0] = key;
                     s_nr = 1;
@@ -172,8 +200,10 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
             const int avail = s_nf - s_head;
             int stop = 0;
             if (avail <= 0) {
+                // entries dropped earlier would still sit in an unbounded
+                // candidate queue: then this is the distance stop
                 stop = 1;
-                s_exh = 1;
+                s_exh = s_dropped ? 0 : 1;
             } else if (s_visited >= a.max_visited) {
                 stop = 1;
                 s_exh = 1;
@@ -182,9 +212,8 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
             }
             s_stop = stop;
             if (!stop) {
-                int w = avail >> 6;
-                if (w < 4) w = 4;
-                if (w > a.wmax) w = a.wmax;
+                // wide steps: the per-step cost is latency, not work
+                int w = a.wmax;
                 if (w > avail) w = avail;
                 const bool full = s_nr >= ef;
                 const float worst = full ? key_dist(rs0[s_cur_r * G_RC + ef - 1]) : 0.f;
@@ -192,13 +221,12 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
                 for (int i = 0; i < w; i++) {
                     const uint64_t k = F[s_head + i];
                     if (i > 0 && full && key_dist(k) > worst) break;
-                    s_sel[n++] = key_row(k);
+                    s_sel[n++] = grow_of(k);
                 }
                 s_head += n;
                 s_nsel = n;
                 s_nnew = 0;
                 s_nfk = 0;
-                s_nrk = 0;
                 s_steps++;
             }
         }
@@ -209,11 +237,13 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         const int nsel = s_nsel;
         const int dc = a.deg_cap;
         for (int t = tid; t < nsel * dc; t += blockDim.x) {
-            const int s = t / dc, i = t - s * dc;
+            const int s = a.dc_shift >= 0 ? t >> a.dc_shift : t / dc;
+            const int i = t - s * dc;
             const uint32_t node = s_sel[s];
-            if (i >= (int)a.deg[node]) continue;
-            const uint32_t nb = a.adj[(uint64_t)node * dc + i];
-            if (nb >= a.nrows) continue;
+            // both loads in flight at once (the list is allocated to deg_cap)
+            const int dg = (int)__ldg(a.deg + node);
+            const uint32_t nb = __ldg(a.adj + (uint64_t)node * dc + i);
+            if (i >= dg || nb >= a.nrows) continue;
             bool fresh;
             if (s_spilled) {
                 const uint32_t m = 1u << (nb & 31);
@@ -235,83 +265,192 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         const int nnew = s_nnew;
         if (tid == 0) s_visited += (unsigned long long)nnew;
 
-        // ---- distances: 8 lanes per node, 32 nodes per pass
+        // ---- distances: 4 lanes per node, two nodes per lane group, so
+        // 128 rows (64 KB at d=128) are in flight per pass; the predicate
+        // word of each row is fetched with the row. Admission as the
+        // reference cursor: a node enters the frontier while results are
+        // short or it beats the worst result (engine.cpp:1684-1690).
         const bool full = s_nr >= ef;
         const float worst = full ? key_dist(rs0[s_cur_r * G_RC + ef - 1]) : 0.f;
         {
-            const int grp = tid >> 3, sub = tid & 7;
-            for (int base = 0; base < nnew; base += G_THREADS / 8) {
-                const int i = base + grp;
-                const bool ok = i < nnew;
-                const uint32_t node = ok ? nid[i] : 0;
-                float acc = 0.f;
-                if (ok) {
-                    const float *x = a.vecs + (uint64_t)node * a.dpad;
-                    for (int j = sub * 4; j < a.dpad; j += 32) {
-                        float4 v = __ldg((const float4 *)(x + j));
-                        float4 w = *(const float4 *)(sq + j);
-                        float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
-                        acc = fmaf(d0, d0, acc); acc = fmaf(d1, d1, acc);
-                        acc = fmaf(d2, d2, acc); acc = fmaf(d3, d3, acc);
+            constexpr int GROUPS = G_THREADS / 4;
+            const int grp = tid >> 2, sub = tid & 3;
+            for (int base = 0; base < nnew; base += 2 * GROUPS) {
+                const int i0 = base + grp, i1 = i0 + GROUPS;
+                const bool ok0 = i0 < nnew, ok1 = i1 < nnew;
+                // rows past nnew re-read row nid[0] (valid) and are discarded
+                const uint32_t n0 = nid[ok0 ? i0 : 0], n1 = nid[ok1 ? i1 : 0];
+                const float *x0 = a.vecs + (uint64_t)n0 * a.dpad;
+                const float *x1 = a.vecs + (uint64_t)n1 * a.dpad;
+                const uint32_t pw0 = bm ? __ldg(bm + (n0 >> 5)) : ~0u;
+                const uint32_t pw1 = bm ? __ldg(bm + (n1 >> 5)) : ~0u;
+                float acc0 = 0.f, acc1 = 0.f;
+                // chunks of 64 dims: all 8 loads of a chunk issue before use
+                for (int c = 0; c < a.dpad; c += 64) {
+                    float4 v0[4], v1[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int j = c + u * 16 + sub * 4;
+                        const bool in = j < a.dpad;
+                        v0[u] = in ? __ldg((const float4 *)(x0 + j)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        v1[u] = in ? __ldg((const float4 *)(x1 + j)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int j = c + u * 16 + sub * 4;
+                        if (j >= a.dpad) break;
+                        const float4 w = *(const float4 *)(sq + j);
+                        float d0 = v0[u].x - w.x, d1 = v0[u].y - w.y, d2 = v0[u].z - w.z,
+                              d3 = v0[u].w - w.w;
+                        acc0 = fmaf(d0, d0, acc0); acc0 = fmaf(d1, d1, acc0);
+                        acc0 = fmaf(d2, d2, acc0); acc0 = fmaf(d3, d3, acc0);
+                        d0 = v1[u].x - w.x; d1 = v1[u].y - w.y; d2 = v1[u].z - w.z;
+                        d3 = v1[u].w - w.w;
+                        acc1 = fmaf(d0, d0, acc1); acc1 = fmaf(d1, d1, acc1);
+                        acc1 = fmaf(d2, d2, acc1); acc1 = fmaf(d3, d3, acc1);
                     }
                 }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                if (ok && sub == 0 && (!full || acc < worst)) {
-                    const uint64_t key = make_key(acc, node);
-                    nfk[atomicAdd(&s_nfk, 1)] = key;
-                    bool pass = true;
-                    if (bm) {
-                        atomicAdd(&s_probes, 1u);
-                        pass = (__ldg(bm + (node >> 5)) >> (node & 31)) & 1u;
+#pragma unroll
+                for (int o = 2; o; o >>= 1) {
+                    acc0 += __shfl_xor_sync(0xffffffffu, acc0, o);
+                    acc1 += __shfl_xor_sync(0xffffffffu, acc1, o);
+                }
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const bool ok = r ? ok1 : ok0;
+                    const float acc = r ? acc1 : acc0;
+                    const uint32_t node = r ? n1 : n0;
+                    if (ok && sub == 0 && (!full || acc < worst)) {
+                        const bool pass = ((r ? pw1 : pw0) >> (node & 31)) & 1u;
+                        if (bm) atomicAdd(&s_probes, 1u);
+                        const int slot = atomicAdd(&s_nfk, 1);
+                        nfk[slot] = make_key(acc, node | (pass ? G_PASS : 0u));
                     }
-                    if (pass) nrk[atomicAdd(&s_nrk, 1)] = key;
                 }
             }
         }
         __syncthreads();
-        const int nnf = s_nfk, nnr = s_nrk;
+        const int nnf = s_nfk;
 
-        // ---- sort the step's new entries
-        int n2 = 1;
-        while (n2 < (nnf > nnr ? nnf : nnr)) n2 <<= 1;
-        for (int i = tid; i < n2; i += blockDim.x) {
-            if (i >= nnf) nfk[i] = KEY_MAX;
-            if (i >= nnr) nrk[i] = KEY_MAX;
+        // ---- sort the step's new keys, then merge them by rank: a new
+        // key's place is its index among the sorted new keys plus a binary
+        // search in the old list, and an old entry moves up by the number
+        // of new keys placed before it (keys are unique: each node is
+        // visited once).
+        {
+            int n2 = 64;
+            while (n2 < nnf) n2 <<= 1;
+            for (int i = nnf + tid; i < n2; i += blockDim.x) nfk[i] = KEY_MAX;
+            __syncthreads();
+            block_sort_pairs(nfk, salt, n2);
+            __syncthreads();
         }
-        __syncthreads();
-        if (n2 > 1) {
-            // both arrays share the network (two independent sorts)
-            for (int k = 2; k <= n2; k <<= 1) {
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    for (int it = tid; it < n2; it += blockDim.x) {
-                        uint64_t *buf = it < (n2 >> 1) ? nfk : nrk;
-                        const int i = it < (n2 >> 1) ? it : it - (n2 >> 1);
-                        const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-                        const int hi = lo | j;
-                        const uint64_t x = buf[lo], y = buf[hi];
-                        if ((x > y) == ((lo & k) == 0)) {
-                            buf[lo] = y;
-                            buf[hi] = x;
-                        }
-                    }
-                    __syncthreads();
-                }
+        // exclusive prefix of the pass bits over the sorted keys (thread t
+        // owns sorted positions 2t, 2t + 1)
+        const int i0 = 2 * tid;
+        const uint64_t k0 = i0 < nnf ? nfk[i0] : KEY_MAX;
+        const uint64_t k1 = i0 + 1 < nnf ? nfk[i0 + 1] : KEY_MAX;
+        const int p0 = (i0 < nnf && ((uint32_t)k0 & G_PASS)) ? 1 : 0;
+        const int p1 = (i0 + 1 < nnf && ((uint32_t)k1 & G_PASS)) ? 1 : 0;
+        int incl = p0 + p1;
+        {
+            const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
             }
+            if (lane == 31) s_wpass[warp] = incl;
+            __syncthreads();
+            for (int w = 0; w < warp; w++) incl += s_wpass[w];
         }
-
-        // ---- merge into frontier and results (ping-pong buffers)
+        int nnr = 0;
+        for (int w = 0; w < G_THREADS / 32; w++) nnr += s_wpass[w];
         const int cf = s_cur_f, cr = s_cur_r;
         const int head = s_head, nf = s_nf, nr = s_nr;
-        merge_path(fr0 + cf * G_FC + head, nf - head, nfk, nnf, fr0 + (cf ^ 1) * G_FC, G_FC);
-        merge_path(rs0 + cr * G_RC, nr, nrk, nnr, rs0 + (cr ^ 1) * G_RC, ef);
+        const uint64_t *Rold = rs0 + cr * G_RC;
+        uint64_t *Rnew = rs0 + (cr ^ 1) * G_RC;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            if (!(e ? p1 : p0)) continue;
+            const uint64_t key = e ? k1 : k0;
+            const int rr = incl - (e ? 1 : p1 + 1);  // exclusive rank among passing keys
+            int lo = 0, hi = nr;  // first old result > key
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (Rold[mid] < key) lo = mid + 1; else hi = mid;
+            }
+            rpos[rr] = lo;
+            if (rr + lo < ef) Rnew[rr + lo] = key;
+        }
+        __syncthreads();
+        for (int i = tid; i < nr; i += blockDim.x) {
+            int lo = 0, hi = nnr;  // new results placed at or before i
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (rpos[mid] <= i) lo = mid + 1; else hi = mid;
+            }
+            if (i + lo < ef) Rnew[i + lo] = Rold[i];
+        }
+        __syncthreads();
+        // frontier entries beyond the worst of a full result list are never
+        // expanded (the stop test would end the search first): drop them
+        const int nr2 = min(nr + nnr, ef);
+        const uint64_t kthr =
+            nr2 >= ef ? (((uint64_t)__float_as_uint(key_dist(Rnew[ef - 1])) << 32) | 0xFFFFFFFFull)
+                      : KEY_MAX;
+        const uint64_t *Fold = fr0 + cf * G_FC + head;
+        uint64_t *Fnew = fr0 + (cf ^ 1) * G_FC;
+        int na, nk;
+        {
+            int lo = 0, hi = nf - head;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (Fold[mid] <= kthr) lo = mid + 1; else hi = mid;
+            }
+            na = lo;
+            lo = 0;
+            hi = nnf;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (nfk[mid] <= kthr) lo = mid + 1; else hi = mid;
+            }
+            nk = lo;
+        }
+        for (int s = tid; s < nk; s += blockDim.x) {
+            const uint64_t key = nfk[s];
+            int lo = 0, hi = na;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (Fold[mid] < key) lo = mid + 1; else hi = mid;
+            }
+            fpos[s] = lo;
+            if (s + lo < G_FC) Fnew[s + lo] = key;
+        }
+        __syncthreads();
+        {
+            const int chunk = (na + G_THREADS - 1) / G_THREADS;
+            const int a0 = tid * chunk, a1 = min(a0 + chunk, na);
+            if (a0 < a1) {
+                int lo = 0, hi = nk;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (fpos[mid] <= a0) lo = mid + 1; else hi = mid;
+                }
+                int sft = lo;
+                for (int i = a0; i < a1; i++) {
+                    while (sft < nk && fpos[sft] <= i) sft++;
+                    if (i + sft < G_FC) Fnew[i + sft] = Fold[i];
+                }
+            }
+        }
         __syncthreads();
         if (tid == 0) {
-            s_nf = min(nf - head + nnf, G_FC);
+            if (na < nf - head || nk < nnf || na + nk > G_FC) s_dropped = 1;
+            s_nf = min(na + nk, G_FC);
             s_head = 0;
             s_cur_f = cf ^ 1;
-            s_nr = min(nr + nnr, ef);
+            s_nr = nr2;
             s_cur_r = cr ^ 1;
         }
 
@@ -335,9 +474,9 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
     const uint64_t *R = rs0 + s_cur_r * G_RC;
     for (int i = tid; i < nr; i += blockDim.x) {
         FvHit h;
-        h.node = key_row(R[i]);
+        h.node = grow_of(R[i]);
         h.dist = key_dist(R[i]);
-        a.out[(uint64_t)q * ef + i] = h;
+        a.out[(uint64_t)q * a.ef + i] = h;
     }
     if (tid == 0) {
         a.out_cnt[q] = (uint32_t)nr;
@@ -352,7 +491,7 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
 }
 
 size_t graph_smem_bytes(int dpad) {
-    return (size_t)(2 * G_FC + 2 * G_RC + 2 * G_NB) * 8 + (size_t)(G_HC + G_NB) * 4 +
+    return (size_t)(2 * G_FC + 2 * G_RC + 2 * G_NB) * 8 + (size_t)(G_HC + 3 * G_NB) * 4 +
            (size_t)dpad * 4;
 }
 
@@ -379,6 +518,10 @@ extern "C" int fv_gpu_graph_batch(FvGpuIndex *g, int nq, const float *queries,
         if (errbuf && errlen) snprintf(errbuf, errlen, "gpu: graph not uploaded");
         return -1;
     }
+    if (g->count >= (1ull << 31)) {  // keys keep the predicate bit in bit 31 of the row
+        if (errbuf && errlen) snprintf(errbuf, errlen, "gpu: graph search needs < 2^31 rows");
+        return -1;
+    }
     if (nq < 1 || nq > FV_GPU_MAX_BATCH || ef < 1 || ef > FV_GPU_MAX_EF || !queries || !qd ||
         !out || !out_cnt || !exhausted) {
         if (errbuf && errlen) snprintf(errbuf, errlen, "gpu: bad graph batch (nq=%d ef=%u)", nq, ef);
@@ -397,6 +540,54 @@ extern "C" int fv_gpu_graph_batch(FvGpuIndex *g, int nq, const float *queries,
 }
 
 namespace pv {
+
+GraphOut graph_out_layout(int nq, uint32_t ef) {
+    GraphOut lo;
+    const size_t hit_bytes = (size_t)nq * ef * sizeof(FvHit);
+    lo.off_cnt = (hit_bytes + 255) & ~(size_t)255;
+    lo.off_exh = lo.off_cnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
+    lo.off_st = lo.off_exh + (((size_t)nq + 255) & ~(size_t)255);
+    lo.bytes = lo.off_st + (size_t)nq * 16;
+    return lo;
+}
+
+int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entries,
+                 const int32_t *d_qprog, const uint16_t *d_efq, uint32_t ef,
+                 uint64_t max_visited, char *od, const GraphOut &lo, char *errbuf,
+                 size_t errlen) {
+    const uint64_t bm_words = (g->count + 31) / 32;
+    GraphScratch &gs = g->graph;
+    PV_CUDA_OK(gs.visited.ensure((size_t)nq * bm_words * 4), errbuf, errlen);
+    GraphArgs a;
+    a.vecs = g->d_vecs;
+    a.dpad = g->dpad;
+    a.nrows = g->count;
+    a.adj = g->d_adj;
+    a.deg = g->d_deg;
+    a.deg_cap = g->deg_cap;
+    a.dc_shift = -1;
+    for (int sh = 0; sh < 16; sh++)
+        if (g->deg_cap == (1 << sh)) a.dc_shift = sh;
+    a.queries = d_q;
+    a.entries = d_entries;
+    a.qprog = d_qprog;
+    a.bitmaps = g->scan.bitmaps.as<uint32_t>();
+    a.bm_words = bm_words;
+    a.ef = (int)ef;
+    a.efq = d_efq;
+    a.max_visited = max_visited;
+    int wmax = G_NB / (g->deg_cap > 0 ? g->deg_cap : 1);
+    if (wmax > 16) wmax = 16;
+    if (wmax < 1) wmax = 1;
+    a.wmax = wmax;
+    a.visited_bits = gs.visited.as<uint32_t>();
+    a.out = (FvHit *)od;
+    a.out_cnt = (uint32_t *)(od + lo.off_cnt);
+    a.out_exh = (uint8_t *)(od + lo.off_exh);
+    a.stats = (uint32_t *)(od + lo.off_st);
+    PV_CUDA_OK(launch_graph(a, nq, g->stream), errbuf, errlen);
+    return 0;
+}
 
 int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
                    const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,
@@ -417,7 +608,6 @@ int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *
     char *d = db.stage_d->as<char>();
     const uint64_t bm_words = (g->count + 31) / 32;
     ScanScratch &s = g->scan;
-    GraphScratch &gs = g->graph;
     const int P = db.P;
     cudaEventRecord(g->ev0, g->stream);
     if (P > 0) {
@@ -431,40 +621,16 @@ int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *
                                   db.ninsns, db.nconsts),
                    errbuf, errlen);
     }
-    PV_CUDA_OK(gs.visited.ensure((size_t)nq * bm_words * 4), errbuf, errlen);
-    const size_t hit_bytes = (size_t)nq * ef * sizeof(FvHit);
-    const size_t off_cnt = (hit_bytes + 255) & ~(size_t)255;
-    const size_t off_exh = off_cnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
-    const size_t off_st = off_exh + (((size_t)nq + 255) & ~(size_t)255);
-    const size_t obytes = off_st + (size_t)nq * 16;
+    const GraphOut lo = graph_out_layout(nq, ef);
+    const size_t off_cnt = lo.off_cnt, off_exh = lo.off_exh, off_st = lo.off_st;
+    const size_t obytes = lo.bytes;
     PV_CUDA_OK(s.out_d.ensure(obytes), errbuf, errlen);
     PV_CUDA_OK(s.out_h.ensure(obytes), errbuf, errlen);
     char *od = s.out_d.as<char>();
-
-    GraphArgs a;
-    a.vecs = g->d_vecs;
-    a.dpad = g->dpad;
-    a.nrows = g->count;
-    a.adj = g->d_adj;
-    a.deg = g->d_deg;
-    a.deg_cap = g->deg_cap;
-    a.queries = (const float *)(d + db.off_q);
-    a.entries = (const uint32_t *)(d + off_ent);
-    a.qprog = (const int32_t *)(d + db.off_qprog);
-    a.bitmaps = s.bitmaps.as<uint32_t>();
-    a.bm_words = bm_words;
-    a.ef = (int)ef;
-    a.max_visited = max_visited;
-    int wmax = G_NB / (g->deg_cap > 0 ? g->deg_cap : 1);
-    if (wmax > 16) wmax = 16;
-    if (wmax < 1) wmax = 1;
-    a.wmax = wmax;
-    a.visited_bits = gs.visited.as<uint32_t>();
-    a.out = (FvHit *)od;
-    a.out_cnt = (uint32_t *)(od + off_cnt);
-    a.out_exh = (uint8_t *)(od + off_exh);
-    a.stats = (uint32_t *)(od + off_st);
-    PV_CUDA_OK(launch_graph(a, nq, g->stream), errbuf, errlen);
+    if (graph_launch(g, nq, (const float *)(d + db.off_q), (const uint32_t *)(d + off_ent),
+                     (const int32_t *)(d + db.off_qprog), nullptr, ef, max_visited, od, lo,
+                     errbuf, errlen))
+        return -1;
     cudaEventRecord(g->ev1, g->stream);
     PV_CUDA_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream), errbuf,
                errlen);

@@ -178,7 +178,7 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
     Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
                    &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
                    &g->scan.out_d, &g->scan.out_h, &g->graph.visited, &g->graph.res,
-                   &g->graph.stats};
+                   &g->graph.stats, &g->graph.route};
     for (Buf *b : bufs) b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);

@@ -65,6 +65,7 @@ struct GraphScratch {
     Buf visited;  // per query overflow bitmap (words), zeroed by the kernel
     Buf res;      // per query results
     Buf stats;    // per query counters
+    Buf route;    // routed batches: features, logits, beam widths
 };
 
 }  // namespace pv

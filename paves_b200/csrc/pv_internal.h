@@ -69,10 +69,11 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
                   DevBatch &db, size_t extra_bytes, char *errbuf, size_t errlen);
 int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen);
 // ev (optional): 5 events recorded before bitmaps, before scan, after scan,
-// after re-rank and after merge.
+// after re-rank and after merge. bitmaps_ready: the batch's bitmaps and
+// popcounts are already in g->scan (no bitmap launch).
 int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
                  uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
-                 cudaEvent_t *ev = nullptr);
+                 cudaEvent_t *ev = nullptr, bool bitmaps_ready = false);
 int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
                    uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt,
                    uint8_t *truncated, char *errbuf, size_t errlen);
@@ -91,6 +92,18 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);
 
 // ---- graph search (graph.cu)
+// ---- graph search (graph.cu)
+struct GraphOut {
+    size_t off_cnt, off_exh, off_st, bytes;  // hits at 0, then counts, exhausted, stats
+};
+GraphOut graph_out_layout(int nq, uint32_t ef);
+// Launches the beam search of nq staged queries on g's stream (bitmaps of
+// the batch already in g->scan.bitmaps); d_efq (optional) gives per-query
+// ef <= ef; outputs land in od with layout lo.
+int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entries,
+                 const int32_t *d_qprog, const uint16_t *d_efq, uint32_t ef,
+                 uint64_t max_visited, char *od, const GraphOut &lo, char *errbuf,
+                 size_t errlen);
 int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
                    const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,
                    uint32_t *out_cnt, uint8_t *exhausted, char *errbuf, size_t errlen);
