@@ -2,17 +2,22 @@
 """Benchmark of the PAVES GPU search path on B200.
 
 Workload (synthetic, seeded; stands in for SIFT1M): N = 1,000,000 rows x
-128 dims from the Gaussian-mixture generator, two attribute columns,
-batches of 64 queries whose predicates rotate through the six selectivity
-classes (0.1% .. 95%), filtered L2 top-10. A step is one batch through the
-device: predicate bitmaps, scan, merge.
+128 dims from the Gaussian-mixture generator, two attribute columns, an
+HNSW graph (M=16, efConstruction=200) built by the library, and six
+batches of 64 queries, one per filter class (0.1% .. 95% selectivity),
+filtered L2 top-10. A step is one batch; steps rotate through the classes.
 
-  value     queries/s with inputs resident in HBM, device time (CUDA events
-            on the library's stream) of K back-to-back steps, max over ranks
-  e2e       the same batch through the drop-in C ABI (fv_gpu_brute_batch)
-            with host buffers: predicate compile + H2D + kernels + D2H
-  roofline  the scan kernel: algorithmic bytes (rows once per batch) over
-            its average CUDA-event duration, against MEASURED_PEAKS.json
+  value     chosen path: the learned router (features + MLP on the device)
+            sends each batch to the BF16 tensor-core scan + exact FP32
+            re-rank, or to the graph search at a per-query beam width
+            (pv_routed_batch); queries/s over the device time of K steps
+            (bitmaps, routing, search), max over ranks
+  plain_gpu the exact FP32 scan of the same batches (prepared, resident)
+  e2e       the chosen path through the C ABI with host buffers: predicate
+            compile + H2D + kernels + D2H, wall clock
+  roofline  the tensor-core scan kernel: algorithmic bytes (rows once per
+            batch) over its average CUDA-event duration, against
+            MEASURED_PEAKS.json
   cpu_baseline  the reference engine's CPU BruteCursor (oracle/_ref, built
             from the reference sources) on a bounded sample, all host cores
 
@@ -108,11 +113,16 @@ class Clocks:
         return out
 
 
-def make_workload(n=N_ROWS, d=DIM, nq=BATCH):
-    ds = datagen.make_dataset(n, d, nq=nq)
-    kinds = list(datagen.six_predicates().items())
-    preds = [kinds[q % len(kinds)][1] for q in range(nq)]
-    return ds, preds, [kinds[q % len(kinds)][0] for q in range(nq)]
+def make_workload(n=N_ROWS, d=DIM, nb=BATCH):
+    """Data set and the six filter classes; class c owns queries
+    [c * nb, (c + 1) * nb). Returns (ds, classes [(name, pred)], preds per query)."""
+    classes = list(datagen.six_predicates().items())
+    ds = datagen.make_dataset(n, d, nq=nb * len(classes))
+    preds = [classes[q // nb][1] for q in range(nb * len(classes))]
+    return ds, classes, preds
+
+
+ROUTER_FILE = os.path.join(ROOT, "paves_b200", "router_1m128.npz")
 
 
 # ---------------------------------------------------------------- reference CPU
@@ -151,7 +161,7 @@ def reference_cpu_qps(ds, preds, budget_s=20.0, threads=None):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    ds, preds, _ = make_workload()
+    ds, _, preds = make_workload()
     per_step = []
     for _ in range(args.warmup):
         reference_cpu_qps(ds, preds[:8], budget_s=5.0)
@@ -225,9 +235,11 @@ def kernel_case(name, iters):
     """One batch shape run `iters` times (device-resident inputs): the
     small, self-contained program that ncu captures profile."""
     nq, prec, mode, pk = KERNEL_CASES[name]
-    ds, preds, kinds = make_workload(nq=max(nq, 6))
+    ds, classes, _ = make_workload(nb=max(nq, 1))
     if pk is not None:
-        preds = [preds[pk]] * nq
+        preds = [classes[pk][1]] * nq
+    else:
+        preds = [classes[q % len(classes)][1] for q in range(nq)]
     gi = GpuIndex(ds.vectors, ds.cols, precision=prec)
     bp = pred.concat(preds[:nq], N_ROWS)
     b = prepared_batch(gi, ds.queries[:nq], bp, TOPK, mode)
@@ -263,7 +275,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -272,21 +284,57 @@ def main():
             dist.destroy_process_group()
         return
 
-    ds, preds, kinds = make_workload()
-    gi = GpuIndex(ds.vectors, ds.cols, device=local, precision=_lib.FV_GPU_PREC_BF16)
-    bp = pred.concat(preds, N_ROWS)
-    # plain path: exact FP32 scan of the same batch
-    bx = prepared_batch(gi, ds.queries, bp, TOPK, _lib.PV_MODE_EXACT)
-    batch_run(bx, args.warmup)
-    plain_ms, stx = batch_run(bx, args.steps, stages=True)
-    plain_qps = BATCH * args.steps / (plain_ms / 1e3)
-    # chosen path: BF16 tensor-core scan + exact FP32 re-rank of 4k candidates
-    b = prepared_batch(gi, ds.queries, bp, TOPK, _lib.PV_MODE_LOW)
-    batch_run(b, args.warmup)
-    ids_x, _, _, _ = fetch(bx, BATCH, TOPK)
-    ids_l, _, _, _ = fetch(b, BATCH, TOPK)
-    rec = float(np.mean([len(set(ids_x[q].tolist()) & set(ids_l[q].tolist())) / TOPK
-                         for q in range(BATCH)]))
+    ds, classes, preds_all = make_workload()
+    nclass = len(classes)
+    from paves_b200.router import Router, routed_batch
+    from paves_b200.hnsw import build_or_load
+    # rank 0 builds the graph (or reloads this host's cached copy); the
+    # other ranks then load rank 0's copy instead of building their own
+    cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
+    t_build = time.perf_counter()
+    if rank == 0:
+        hnsw = build_or_load(ds.vectors, cache, 16, 200)
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        hnsw = build_or_load(ds.vectors, cache, 16, 200)
+    build_s = time.perf_counter() - t_build
+    gi = GpuIndex(ds.vectors, ds.cols, l0=hnsw.l0, device=local,
+                  precision=_lib.FV_GPU_PREC_BF16)
+    if not os.path.exists(ROUTER_FILE):
+        raise RuntimeError(f"{ROUTER_FILE} missing: train it with "
+                           "python -m paves_b200.router_train --out " + ROUTER_FILE)
+    z = np.load(ROUTER_FILE)
+    router = Router(z["centroids"].astype(np.float32), device=local)
+    router.set_params(z["params"], z["mean"], z["std"])
+    L = _lib.lib()
+    cls = []
+    for c, (name, p) in enumerate(classes):
+        q = np.ascontiguousarray(ds.queries[c * BATCH:(c + 1) * BATCH], np.float32)
+        ent = hnsw.entries(q)
+        bp = pred.concat([p] * BATCH, N_ROWS, entries=ent)
+        cls.append((name, p, q, ent, bp))
+
+    # plain path: exact FP32 scan of each class batch (prepared, resident)
+    plain = []
+    for name, p, q, ent, bp in cls:
+        bx = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_EXACT)
+        batch_run(bx, 3)
+        plain.append(bx)
+    per_class = max(1, args.steps // nclass)
+    plain_ms = 0.0
+    for bx in plain:
+        ms, _ = batch_run(bx, per_class)
+        plain_ms += ms
+    plain_qps = BATCH * per_class * nclass / (plain_ms / 1e3)
+    exact = [fetch(bx, BATCH, TOPK) for bx in plain]
+
+    def routed(c):
+        name, p, q, ent, bp = cls[c]
+        return routed_batch(gi, router, q, [p] * BATCH, TOPK, ent, topb=TOPK)
+
+    for i in range(args.warmup):
+        routed(i % nclass)
 
     def barrier():
         if dist:
@@ -297,101 +345,126 @@ def main():
 
     barrier()
     clk = Clocks(local)
-    total_ms, _ = batch_run(b, args.steps)
+    dev_ms, launches, graph_steps = 0.0, 0, 0
+    results = {}
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        c = i % nclass
+        ids, dists, cnt, dec, ex, st = routed(c)
+        dev_ms += float(st.sum())
+        launches += int(L.pv_last_launches(gi.handle))
+        graph_steps += ex
+        results[c] = (ids, cnt, dec, ex)
+    wall_s = time.perf_counter() - t0
     clocks = clk.stop()
     barrier()
     if dist:
         import torch
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        t = torch.tensor([dev_ms, wall_s], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = BATCH * args.steps * world / (total_ms / 1e3)
+        dev_ms, wall_s = float(t[0].item()), float(t[1].item())
+    ms_per_step = dev_ms / args.steps
+    value = BATCH * args.steps * world / (dev_ms / 1e3)
+    e2e_qps = BATCH * args.steps * world / wall_s
+    recall = {}
+    for c, (name, *_rest) in enumerate(cls):
+        if c not in results:
+            continue
+        ids, cnt, dec, ex = results[c]
+        xi, _, xc, _ = exact[c]
+        r = [np.isin(xi[i, :xc[i]], ids[i, :cnt[i]]).sum() / max(1, int(xc[i]))
+             for i in range(BATCH)]
+        recall[name] = {"recall_at_10": round(float(np.mean(r)), 4),
+                        "path": "graph" if ex else "bf16-scan",
+                        "graph_queries": int((dec > 0).sum())}
 
-    # per-kernel device times of the same steps (events between kernels)
-    _, st = batch_run(b, args.steps, stages=True)
-    superset = int(_lib.lib().pv_last_superset(gi.handle))
-    scan_ms = st[1] / args.steps
+    # the tensor-core scan kernel alone (each class batch, prepared)
+    scan_ms, st_tot, superset = 0.0, [0.0] * 4, 0
+    for name, p, q, ent, bp in cls:
+        b = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_LOW)
+        batch_run(b, 3)
+        _, st = batch_run(b, per_class, stages=True)
+        st_tot = [x + y for x, y in zip(st_tot, st)]
+        superset = int(L.pv_last_superset(gi.handle))
+        L.pv_batch_free(b)
+    nrun = per_class * nclass
+    scan_ms = st_tot[1] / nrun
+    scan_only_qps = BATCH * nrun / (sum(st_tot) / 1e3)
     hbm, bf16, peak_kind = load_peaks()
     # tensor-core scan: bf16 rows (128 dims = 256 B) + f32 norm, once per batch
     alg_bytes = N_ROWS * (DIM * 2 + 4)
     achieved = alg_bytes / (scan_ms / 1e3) / 1e9
-    plain_scan_ms = stx[1] / args.steps
 
     # scan GB/s at batch 1 (the HBM-bound exact scan)
-    bp1 = pred.concat([preds[5]], N_ROWS)
+    bp1 = pred.concat([classes[5][1]], N_ROWS)
     b1 = prepared_batch(gi, ds.queries[:1], bp1, TOPK, _lib.PV_MODE_EXACT)
     batch_run(b1, 3)
     _, st1 = batch_run(b1, 20, stages=True)
     scan1_ms = st1[1] / 20
     scan_gbs_b1 = N_ROWS * DIM * 4 / (scan1_ms / 1e3) / 1e9
-    _lib.lib().pv_batch_free(b1)
+    L.pv_batch_free(b1)
 
-    # end to end through the drop-in ABI, host buffers
-    q = np.ascontiguousarray(ds.queries, np.float32)
-    for _ in range(3):
-        gi.brute_batch_raw(q, bp, TOPK)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        gi.brute_batch_raw(q, bp, TOPK)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        import torch
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_qps = BATCH * args.steps * world / e2e_s
+    # bytes crossing PCIe per step of the chosen path (from the arrays passed)
+    name, p, q, ent, bp = cls[0]
     h2d = q.nbytes + bp.qd.nbytes + bp.nodes.nbytes + bp.children.nbytes + bp.invals.nbytes
-    d2h = BATCH * TOPK * 16 + BATCH * 4 + BATCH
+    d2h = BATCH * TOPK * 16 + BATCH * 4 + BATCH * 2
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import refengine
             if refengine.available("cpu"):
-                qps, nrun, threads = reference_cpu_qps(ds, preds, budget_s=15.0)
+                qps, nrun_c, threads = reference_cpu_qps(ds, preds_all, budget_s=15.0)
                 cpu = {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
                        "kind": "reference",
-                       "sample": f"{nrun} queries of the batch, one at a time (BruteCursor)"}
+                       "sample": f"{nrun_c} queries of the six class batches, one at a time "
+                                 "(BruteCursor)"}
         except Exception as e:  # baseline is informative only
             cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"failed: {e}"}
 
-    _lib.lib().pv_batch_free(b)
-    _lib.lib().pv_batch_free(bx)
+    for bx in plain:
+        L.pv_batch_free(bx)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
             "data": "synthetic",
-            "config": {"workload": "1M x 128 Gaussian-mixture rows (integer-valued), 64-query "
-                                   "batches over six predicate classes 0.1%-95%, filtered "
-                                   "top-10; BF16 tensor-core scan + exact FP32 re-rank",
+            "config": {"workload": "1M x 128 Gaussian-mixture rows (integer-valued), six "
+                                   "64-query batches, one per filter class (0.1%-95%), "
+                                   "filtered top-10; learned router over the BF16 "
+                                   "tensor-core scan + exact FP32 re-rank and the HNSW "
+                                   "graph search",
                        "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK,
-                       "rerank_candidates": superset,
-                       "path": "bf16-scan", "l2_flush": "inputs larger than L2 (256 MB bf16 "
-                                                        "rows, 512 MB f32 rows vs 126 MB)"},
-            "recall_at_10_vs_exact": round(rec, 4),
+                       "rerank_candidates": superset, "hnsw": "M=16 efC=200",
+                       "l2_flush": "inputs larger than L2 (256 MB bf16 rows, 512 MB f32 "
+                                   "rows vs 126 MB)"},
+            "recall_per_class": recall,
+            "recall_at_10_min": round(min(v["recall_at_10"] for v in recall.values()), 4),
+            "graph_batches": graph_steps,
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
-                          "path": "exact FP32 scan", "scan_ms": round(plain_scan_ms, 4)},
+                          "path": "exact FP32 scan"},
+            "scan_only": {"value": round(scan_only_qps, 1), "unit": "queries/s",
+                          "path": "bf16 scan + re-rank, no router"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(achieved / hbm, 4),
                          "traffic": load_traffic("scan_tc_kernel"),
                          "kernel": "scan_tc_kernel", "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
             "scan_gbs_batch1": round(scan_gbs_b1, 1),
-            "stage_ms": {"bitmap+prep+seed": round(st[0] / args.steps, 4),
+            "stage_ms": {"bitmap+prep+seed": round(st_tot[0] / nrun, 4),
                          "scan": round(scan_ms, 4),
-                         "merge+rerank": round(st[2] / args.steps, 4)},
+                         "merge+rerank": round(st_tot[2] / nrun, 4)},
+            "hnsw_build_s": round(build_s, 1),
             "clocks": clocks,
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            # per step: bitmap, query prep, tensor-core scan, merge, re-rank
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": launches,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
+    router.close()
     gi.close()
     if dist:
         dist.barrier()

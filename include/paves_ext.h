@@ -260,6 +260,10 @@ float pv_last_kernel_ms(const FvGpuIndex *g);
  * exact: integer rows and queries with all sums below 2^24); 0 if none. */
 int pv_last_superset(const FvGpuIndex *g);
 
+/* Kernels launched by the last batch call on g (summed over the iterations
+ * of pv_batch_run). */
+int pv_last_launches(const FvGpuIndex *g);
+
 /* Counters of the last fv_gpu_graph_batch call: per query [steps, visited,
  * predicate probes, results]; copies min(nq, last nq) rows, returns rows. */
 int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq);

@@ -101,6 +101,7 @@ _EXT_SIGS = {
                                   P, C.c_int]),
     "pv_last_kernel_ms": (C.c_float, [P]),
     "pv_last_superset": (C.c_int, [P]),
+    "pv_last_launches": (C.c_int, [P]),
     "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
 }
 PV_MODE_EXACT, PV_MODE_LOW = 0, 1

@@ -86,6 +86,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else if (P > 0) {
         PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
         PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
+        g->launches++;
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
                                   s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
@@ -133,6 +134,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     a.part = s.part.as<uint64_t>();
     a.part_cnt = s.part_cnt.as<uint32_t>();
     if (ev) cudaEventRecord(ev[1], g->stream);
+    g->launches += 2;  // scan + merge
     PV_CUDA_OK(launch_scan_f32(a, pl, g->stream), errbuf, errlen);
     if (ev) {
         cudaEventRecord(ev[2], g->stream);
@@ -189,6 +191,7 @@ namespace pv {
 int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
                    uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
                    char *errbuf, size_t errlen) {
+    g->launches = 0;
     DevBatch db;
     db.stage_h = &g->scan.stage_h;
     db.stage_d = &g->scan.stage_d;

@@ -90,6 +90,7 @@ extern "C" int pv_batch_run(PvBatch *b, int iters, float *stage_ms, float *total
     FvGpuIndex *g = b->g;
     std::lock_guard<std::mutex> lk(g->mu);
     PV_CUDA_OK(cudaSetDevice(g->device), errbuf, errlen);
+    g->launches = 0;
     char *od = b->out_d.as<char>();
     float st[4] = {0, 0, 0, 0}, tot = 0.f;
     if (stage_ms) {
@@ -160,6 +161,8 @@ extern "C" void pv_batch_free(PvBatch *b) {
 extern "C" float pv_last_kernel_ms(const FvGpuIndex *g) { return g ? g->last_kernel_ms : 0.f; }
 
 extern "C" int pv_last_superset(const FvGpuIndex *g) { return g ? g->last_superset : 0; }
+
+extern "C" int pv_last_launches(const FvGpuIndex *g) { return g ? g->launches : 0; }
 
 extern "C" int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq) {
     if (!g || !out) return 0;

@@ -32,7 +32,7 @@
 namespace pv {
 
 constexpr int G_THREADS = 256;
-constexpr int G_HC = 4096;   // visited hash slots (u32)
+constexpr int G_HC = 8192;   // visited hash slots (u32)
 constexpr int G_FC = 8192;   // frontier capacity (selective filters grow it)
 constexpr int G_RC = 512;    // result capacity (FV_GPU_MAX_EF)
 constexpr int G_NB = 512;    // new entries per step (W * deg_cap <= G_NB)
@@ -194,40 +194,37 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
     __syncthreads();
 
     for (;;) {
-        // ---- stop tests and selection (thread 0; frontier is ascending)
-        if (tid == 0) {
-            const uint64_t *F = (fr0 + s_cur_f * G_FC);
-            const int avail = s_nf - s_head;
+        // ---- stop tests and selection (warp 0; the frontier is ascending):
+        // the best W entries, cut at the first one beyond the worst result
+        if (tid < 32) {
+            const int lane = tid;
+            const uint64_t *F = fr0 + s_cur_f * G_FC;
+            const int head = s_head, avail = s_nf - head;
+            const bool full = s_nr >= ef;
+            const float worst = full ? key_dist(rs0[s_cur_r * G_RC + ef - 1]) : 0.f;
+            const int w = avail < a.wmax ? avail : a.wmax;
+            const uint64_t k = lane < w ? F[head + lane] : KEY_MAX;
+            const bool ok = lane < w && (lane == 0 || !full || !(key_dist(k) > worst));
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            const int n = m == 0xffffffffu ? 32 : __ffs(~m) - 1;  // leading run of ok lanes
             int stop = 0;
-            if (avail <= 0) {
-                // entries dropped earlier would still sit in an unbounded
-                // candidate queue: then this is the distance stop
-                stop = 1;
-                s_exh = s_dropped ? 0 : 1;
-            } else if (s_visited >= a.max_visited) {
-                stop = 1;
-                s_exh = 1;
-            } else if (s_nr >= ef && key_dist(F[s_head]) > key_dist(rs0[s_cur_r * G_RC + ef - 1])) {
-                stop = 1;
-            }
-            s_stop = stop;
-            if (!stop) {
-                // wide steps: the per-step cost is latency, not work
-                int w = a.wmax;
-                if (w > avail) w = avail;
-                const bool full = s_nr >= ef;
-                const float worst = full ? key_dist(rs0[s_cur_r * G_RC + ef - 1]) : 0.f;
-                int n = 0;
-                for (int i = 0; i < w; i++) {
-                    const uint64_t k = F[s_head + i];
-                    if (i > 0 && full && key_dist(k) > worst) break;
-                    s_sel[n++] = grow_of(k);
+            if (avail <= 0) stop = 1;
+            else if (s_visited >= a.max_visited) stop = 2;
+            else if (full && key_dist(F[head]) > worst) stop = 3;
+            if (!stop && lane < n) s_sel[lane] = grow_of(k);
+            if (lane == 0) {
+                s_stop = stop;
+                // an empty frontier is exhaustion unless entries were dropped
+                // (they would still sit in an unbounded candidate queue)
+                if (stop == 1) s_exh = s_dropped ? 0 : 1;
+                if (stop == 2) s_exh = 1;
+                if (!stop) {
+                    s_head = head + n;
+                    s_nsel = n;
+                    s_nnew = 0;
+                    s_nfk = 0;
+                    s_steps++;
                 }
-                s_head += n;
-                s_nsel = n;
-                s_nnew = 0;
-                s_nfk = 0;
-                s_steps++;
             }
         }
         __syncthreads();
@@ -236,30 +233,43 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         // ---- gather neighbours of the selected nodes, visited test-and-set
         const int nsel = s_nsel;
         const int dc = a.deg_cap;
-        for (int t = tid; t < nsel * dc; t += blockDim.x) {
-            const int s = a.dc_shift >= 0 ? t >> a.dc_shift : t / dc;
-            const int i = t - s * dc;
-            const uint32_t node = s_sel[s];
-            // both loads in flight at once (the list is allocated to deg_cap)
-            const int dg = (int)__ldg(a.deg + node);
-            const uint32_t nb = __ldg(a.adj + (uint64_t)node * dc + i);
-            if (i >= dg || nb >= a.nrows) continue;
-            bool fresh;
-            if (s_spilled) {
-                const uint32_t m = 1u << (nb & 31);
-                fresh = (atomicOr(vb + (nb >> 5), m) & m) == 0;
-            } else {
-                uint32_t h = hash_u32(nb) & (G_HC - 1);
-                fresh = false;
-                for (int probe = 0; probe < G_HC; probe++) {
-                    const uint32_t old = atomicCAS(hash + h, G_EMPTY, nb);
-                    if (old == G_EMPTY) { fresh = true; break; }
-                    if (old == nb) break;
-                    h = (h + 1) & (G_HC - 1);
+        const int total = nsel * dc;
+        const int lane = tid & 31;
+        for (int base = 0; base < total; base += G_THREADS) {
+            const int t = base + tid;
+            bool fresh = false;
+            uint32_t nb = 0;
+            if (t < total) {
+                const int s = a.dc_shift >= 0 ? t >> a.dc_shift : t / dc;
+                const int i = t - s * dc;
+                const uint32_t node = s_sel[s];
+                // both loads in flight at once (the list is allocated to deg_cap)
+                const int dg = (int)__ldg(a.deg + node);
+                nb = __ldg(a.adj + (uint64_t)node * dc + i);
+                if (i < dg && nb < a.nrows) {
+                    if (s_spilled) {
+                        const uint32_t m = 1u << (nb & 31);
+                        fresh = (atomicOr(vb + (nb >> 5), m) & m) == 0;
+                    } else {
+                        uint32_t h = hash_u32(nb) & (G_HC - 1);
+                        for (int probe = 0; probe < G_HC; probe++) {
+                            const uint32_t old = atomicCAS(hash + h, G_EMPTY, nb);
+                            if (old == G_EMPTY) { fresh = true; break; }
+                            if (old == nb) break;
+                            h = (h + 1) & (G_HC - 1);
+                        }
+                    }
                 }
-                if (fresh) atomicAdd(&s_hcount, 1);
             }
-            if (fresh) nid[atomicAdd(&s_nnew, 1)] = nb;
+            // one shared-memory atomic per warp for the appends
+            const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+            int wb = 0;
+            if (lane == 0 && fm) {
+                wb = atomicAdd(&s_nnew, __popc(fm));
+                if (!s_spilled) atomicAdd(&s_hcount, __popc(fm));
+            }
+            wb = __shfl_sync(0xffffffffu, wb, 0);
+            if (fresh) nid[wb + __popc(fm & ((1u << lane) - 1u))] = nb;
         }
         __syncthreads();
         const int nnew = s_nnew;
@@ -273,59 +283,80 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         const bool full = s_nr >= ef;
         const float worst = full ? key_dist(rs0[s_cur_r * G_RC + ef - 1]) : 0.f;
         {
-            constexpr int GROUPS = G_THREADS / 4;
+            constexpr int GROUPS = G_THREADS / 4;  // lane groups of 4
+            constexpr int RPG = 4;                 // rows per group per pass
             const int grp = tid >> 2, sub = tid & 3;
-            for (int base = 0; base < nnew; base += 2 * GROUPS) {
-                const int i0 = base + grp, i1 = i0 + GROUPS;
-                const bool ok0 = i0 < nnew, ok1 = i1 < nnew;
-                // rows past nnew re-read row nid[0] (valid) and are discarded
-                const uint32_t n0 = nid[ok0 ? i0 : 0], n1 = nid[ok1 ? i1 : 0];
-                const float *x0 = a.vecs + (uint64_t)n0 * a.dpad;
-                const float *x1 = a.vecs + (uint64_t)n1 * a.dpad;
-                const uint32_t pw0 = bm ? __ldg(bm + (n0 >> 5)) : ~0u;
-                const uint32_t pw1 = bm ? __ldg(bm + (n1 >> 5)) : ~0u;
-                float acc0 = 0.f, acc1 = 0.f;
-                // chunks of 64 dims: all 8 loads of a chunk issue before use
+            for (int base = 0; base < nnew; base += RPG * GROUPS) {
+                uint32_t nn[RPG], pw[RPG];
+                bool okr[RPG];
+                const float *xr[RPG];
+                float acc[RPG];
+#pragma unroll
+                for (int r = 0; r < RPG; r++) {
+                    const int i = base + grp + r * GROUPS;
+                    okr[r] = i < nnew;
+                    // rows past nnew re-read row nid[0] (valid) and are discarded
+                    nn[r] = nid[okr[r] ? i : 0];
+                    xr[r] = a.vecs + (uint64_t)nn[r] * a.dpad;
+                    pw[r] = bm ? __ldg(bm + (nn[r] >> 5)) : ~0u;
+                    acc[r] = 0.f;
+                }
+                // chunks of 64 dims: all loads of a chunk issue before use
                 for (int c = 0; c < a.dpad; c += 64) {
-                    float4 v0[4], v1[4];
+                    float4 v[RPG][4];
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         const int j = c + u * 16 + sub * 4;
                         const bool in = j < a.dpad;
-                        v0[u] = in ? __ldg((const float4 *)(x0 + j)) : make_float4(0.f, 0.f, 0.f, 0.f);
-                        v1[u] = in ? __ldg((const float4 *)(x1 + j)) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                        for (int r = 0; r < RPG; r++)
+                            v[r][u] = in ? __ldg((const float4 *)(xr[r] + j))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
                     }
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         const int j = c + u * 16 + sub * 4;
                         if (j >= a.dpad) break;
                         const float4 w = *(const float4 *)(sq + j);
-                        float d0 = v0[u].x - w.x, d1 = v0[u].y - w.y, d2 = v0[u].z - w.z,
-                              d3 = v0[u].w - w.w;
-                        acc0 = fmaf(d0, d0, acc0); acc0 = fmaf(d1, d1, acc0);
-                        acc0 = fmaf(d2, d2, acc0); acc0 = fmaf(d3, d3, acc0);
-                        d0 = v1[u].x - w.x; d1 = v1[u].y - w.y; d2 = v1[u].z - w.z;
-                        d3 = v1[u].w - w.w;
-                        acc1 = fmaf(d0, d0, acc1); acc1 = fmaf(d1, d1, acc1);
-                        acc1 = fmaf(d2, d2, acc1); acc1 = fmaf(d3, d3, acc1);
+#pragma unroll
+                        for (int r = 0; r < RPG; r++) {
+                            const float d0 = v[r][u].x - w.x, d1 = v[r][u].y - w.y;
+                            const float d2 = v[r][u].z - w.z, d3 = v[r][u].w - w.w;
+                            acc[r] = fmaf(d0, d0, acc[r]); acc[r] = fmaf(d1, d1, acc[r]);
+                            acc[r] = fmaf(d2, d2, acc[r]); acc[r] = fmaf(d3, d3, acc[r]);
+                        }
                     }
                 }
 #pragma unroll
-                for (int o = 2; o; o >>= 1) {
-                    acc0 += __shfl_xor_sync(0xffffffffu, acc0, o);
-                    acc1 += __shfl_xor_sync(0xffffffffu, acc1, o);
+                for (int r = 0; r < RPG; r++) {
+                    acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
+                    acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
                 }
+                // admitted rows of this warp (lanes with sub == 0), appended
+                // with one shared-memory atomic per warp
+                unsigned m[RPG];
+                bool ad[RPG];
+                int tot = 0;
 #pragma unroll
-                for (int r = 0; r < 2; r++) {
-                    const bool ok = r ? ok1 : ok0;
-                    const float acc = r ? acc1 : acc0;
-                    const uint32_t node = r ? n1 : n0;
-                    if (ok && sub == 0 && (!full || acc < worst)) {
-                        const bool pass = ((r ? pw1 : pw0) >> (node & 31)) & 1u;
-                        if (bm) atomicAdd(&s_probes, 1u);
-                        const int slot = atomicAdd(&s_nfk, 1);
-                        nfk[slot] = make_key(acc, node | (pass ? G_PASS : 0u));
+                for (int r = 0; r < RPG; r++) {
+                    ad[r] = okr[r] && sub == 0 && (!full || acc[r] < worst);
+                    m[r] = __ballot_sync(0xffffffffu, ad[r]);
+                    tot += __popc(m[r]);
+                }
+                int wb = 0;
+                if (lane == 0 && tot) {
+                    wb = atomicAdd(&s_nfk, tot);
+                    if (bm) atomicAdd(&s_probes, (unsigned)tot);
+                }
+                wb = __shfl_sync(0xffffffffu, wb, 0);
+                const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+                for (int r = 0; r < RPG; r++) {
+                    if (ad[r]) {
+                        const bool pass = (pw[r] >> (nn[r] & 31)) & 1u;
+                        nfk[wb + __popc(m[r] & lt)] = make_key(acc[r], nn[r] | (pass ? G_PASS : 0u));
                     }
+                    wb += __popc(m[r]);
                 }
             }
         }
@@ -337,7 +368,19 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         // search in the old list, and an old entry moves up by the number
         // of new keys placed before it (keys are unique: each node is
         // visited once).
-        {
+        // Up to G_THREADS keys: each thread counts the keys below its own
+        // (independent loads, no barrier chain); more: bitonic sort.
+        uint64_t *srt = nfk;
+        if (nnf <= G_THREADS) {
+            if (tid < nnf) {
+                const uint64_t key = nfk[tid];
+                int r = 0;
+                for (int i = 0; i < nnf; i++) r += nfk[i] < key;
+                salt[r] = key;
+            }
+            srt = salt;
+            __syncthreads();
+        } else {
             int n2 = 64;
             while (n2 < nnf) n2 <<= 1;
             for (int i = nnf + tid; i < n2; i += blockDim.x) nfk[i] = KEY_MAX;
@@ -348,13 +391,13 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
         // exclusive prefix of the pass bits over the sorted keys (thread t
         // owns sorted positions 2t, 2t + 1)
         const int i0 = 2 * tid;
-        const uint64_t k0 = i0 < nnf ? nfk[i0] : KEY_MAX;
-        const uint64_t k1 = i0 + 1 < nnf ? nfk[i0 + 1] : KEY_MAX;
+        const uint64_t k0 = i0 < nnf ? srt[i0] : KEY_MAX;
+        const uint64_t k1 = i0 + 1 < nnf ? srt[i0 + 1] : KEY_MAX;
         const int p0 = (i0 < nnf && ((uint32_t)k0 & G_PASS)) ? 1 : 0;
         const int p1 = (i0 + 1 < nnf && ((uint32_t)k1 & G_PASS)) ? 1 : 0;
         int incl = p0 + p1;
         {
-            const int lane = tid & 31, warp = tid >> 5;
+            const int warp = tid >> 5;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -413,12 +456,12 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
             hi = nnf;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
-                if (nfk[mid] <= kthr) lo = mid + 1; else hi = mid;
+                if (srt[mid] <= kthr) lo = mid + 1; else hi = mid;
             }
             nk = lo;
         }
         for (int s = tid; s < nk; s += blockDim.x) {
-            const uint64_t key = nfk[s];
+            const uint64_t key = srt[s];
             int lo = 0, hi = na;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
@@ -585,6 +628,7 @@ int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entr
     a.out_cnt = (uint32_t *)(od + lo.off_cnt);
     a.out_exh = (uint8_t *)(od + lo.off_exh);
     a.stats = (uint32_t *)(od + lo.off_st);
+    g->launches++;
     PV_CUDA_OK(launch_graph(a, nq, g->stream), errbuf, errlen);
     return 0;
 }
@@ -592,6 +636,7 @@ int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entr
 int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
                    const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,
                    uint32_t *out_cnt, uint8_t *exhausted, char *errbuf, size_t errlen) {
+    g->launches = 0;
     DevBatch db;
     db.stage_h = &g->scan.stage_h;
     db.stage_d = &g->scan.stage_d;
@@ -613,6 +658,7 @@ int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *
     if (P > 0) {
         PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
         PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
+        g->launches++;
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, (const PredInsn *)(d + db.off_insns),
                                   (const PredProg *)(d + db.off_progs),
                                   (const double *)(d + db.off_consts), P,

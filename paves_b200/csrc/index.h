@@ -107,5 +107,6 @@ struct FvGpuIndex {
     int *tc_err = nullptr;  // watchdog word of the last tensor-core scan (device)
     int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels
+    int launches = 0;  // kernels launched by the last call (all iterations)
     std::vector<uint32_t> graph_stats;  // last graph batch: [nq][4] counters
 };

@@ -507,6 +507,7 @@ extern "C" int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const floa
     }
     std::lock_guard<std::mutex> lk(g->mu);
     RT_OK(cudaSetDevice(g->device));
+    g->launches = 0;
     PredBatch pb;
     if (compile_predicates(nq, &qd[0].proot, sizeof(FvGpuQueryDesc), nodes, nnodes, children,
                            nchildren, invals, ninvals, g->ncols, pb, errbuf, errlen) != 0)
@@ -530,6 +531,7 @@ extern "C" int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const floa
     RT_OK(s.popcnt.ensure((size_t)(P > 0 ? P : 1) * 8));
     if (P > 0) {
         RT_OK(s.bitmaps.ensure((size_t)P * bm_words * 4));
+        g->launches++;
         RT_OK(launch_bitmaps(g->d_cols, g->count, (const PredInsn *)(d + db.off_insns),
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
@@ -538,6 +540,7 @@ extern "C" int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const floa
     }
     const size_t fbytes = (size_t)nq * NI * 4;
     RT_OK(s.out_d.ensure(fbytes));
+    g->launches++;
     RT_OK(launch_router_features(r, (const float *)(d + db.off_q), g->dpad, nq,
                                  s.popcnt.as<unsigned long long>(),
                                  (const int32_t *)(d + db.off_qprog), g->count,
@@ -808,6 +811,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     std::unique_lock<std::mutex> lr;
     if (r) lr = std::unique_lock<std::mutex>(r->mu);
     RT_OK(cudaSetDevice(g->device));
+    g->launches = 0;
     PredBatch pb;
     if (compile_predicates(nq, &qd[0].proot, sizeof(FvGpuQueryDesc), nodes, nnodes, children,
                            nchildren, invals, ninvals, g->ncols, pb, errbuf, errlen) != 0)
@@ -846,6 +850,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     RT_OK(s.popcnt.ensure((size_t)(P > 0 ? P : 1) * 8));
     if (P > 0) {
         RT_OK(s.bitmaps.ensure((size_t)P * bm_words * 4));
+        g->launches++;
         RT_OK(launch_bitmaps(g->d_cols, g->count, (const PredInsn *)(d + db.off_insns),
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
@@ -860,6 +865,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     float *dfeat = g->graph.route.as<float>();
     float *dz = (float *)(g->graph.route.as<char>() + fb);
     uint16_t *defq = (uint16_t *)(g->graph.route.as<char>() + fb + zb);
+    g->launches += plan ? 1 : 3;  // (features, MLP,) decision
     if (!plan) {
         RT_OK(launch_router_features(r, (const float *)(d + db.off_q), g->dpad, nq,
                                      s.popcnt.as<unsigned long long>(),

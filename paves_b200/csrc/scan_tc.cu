@@ -605,6 +605,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
     PV_CUDA_OK(cudaMemsetAsync(d_err, 0, 4, g->stream), errbuf, errlen);
 
+    g->launches += 4;  // query prep, main pass, merge, re-rank
     query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
         d_q, nq, g->dpad, g->dim, nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
         fp8 ? (float *)(c + off_qs) : nullptr);
@@ -663,6 +664,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sa.tile0_mul = ntiles_all / grow;
         sa.tile_step = 1;
         sa.tiles_per_cta = 1;
+        g->launches += 2;  // seeding pass + its merge
         PV_CUDA_OK(run(sa), errbuf, errlen);
         ScanPlan sp;
         sp.M = 4096;

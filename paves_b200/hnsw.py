@@ -90,6 +90,8 @@ def build_or_load(vectors: np.ndarray, cache: Optional[str], M: int = 16,
             return h
     h = Hnsw(vectors, M, ef_construction)
     if cache:
-        np.savez(cache, key=key, M=h.M, max_level=h.max_level, entry=h.entry_node, l0=h.l0,
+        tmp = f"{cache}.{os.getpid()}.tmp.npz"
+        np.savez(tmp, key=key, M=h.M, max_level=h.max_level, entry=h.entry_node, l0=h.l0,
                  levels=h.levels, upper_offs=h.upper_offs, upper=h.upper)
+        os.replace(tmp, cache)  # readers never see a partial file
     return h

@@ -316,3 +316,26 @@ def routed_batch(index, router: Optional[Router], queries: np.ndarray, preds, k,
         raise RuntimeError(err.value.decode())
     out = out.reshape(nq, topb)
     return out["node"], out["dist"], cnt, dec, int(ex.value), st
+
+
+def feedback_from_batches(samples) -> Feedback:
+    """The worker's feedback after homogeneous batches (worker.c:296-333
+    attribution: with equal weights in a batch, the per-request sample is
+    the batch time). samples: iterable of (graph?, selectivity, batch_ms, n)."""
+    fb = Feedback.empty()
+    for graph, sel, ms, n in samples:
+        si = 1 if graph else 0
+        b = sel_bucket(int(sel * 1000))
+        us = max(1, int(ms * 1000))
+        for arr, idx, val, alpha in ((fb.q_us[si], b, us, n / (n + 64.0)),
+                                     (fb.batch_us, si, us, 0.125),
+                                     (fb.batch_n16, si, int(n * 16), 0.125)):
+            old = int(arr[idx])
+            arr[idx] = max(1, val if old == 0 else int(old + alpha * (val - old)))
+    return fb
+
+
+def plain_plan(sel: np.ndarray, k, fb: Optional[Feedback] = None) -> np.ndarray:
+    """plain_rule as a pv_routed_batch plan: 0 = scan, else the beam width."""
+    graph, ef = plain_rule(sel, np.broadcast_to(np.asarray(k), np.shape(sel)), fb)
+    return np.where(graph, np.minimum(ef, 512), 0).astype(np.uint16)
