@@ -252,6 +252,41 @@ int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *queries,
                     FvHit *out, uint32_t *out_cnt, uint16_t *decided, int *executed,
                     float *stage_ms, char *errbuf, size_t errlen);
 
+/* ---- stream of uneven micro-batches (no counterpart in the reference) ----
+ * For a serving loop whose batches vary in size, k and filters. At creation
+ * the stream autotunes, per batch-size bucket (1, 2, 4, ... max_batch) and
+ * result-width bucket (16 and max_k, or max_k alone when <= 16), the scan
+ * shape (exact FP32 scan, or the index's reduced-precision tensor-core scan
+ * with its epilogue groups, pipeline stages and CTA count) by timing the
+ * candidates on the sample queries (tune_queries [ntune][dim]); choices are
+ * read from / saved to tune_path (NULL: neither). It then captures one
+ * CUDA graph per bucket: H2D of the staged batch, predicate bitmaps, scan,
+ * merge, re-rank, D2H. pv_stream_run pads a batch to its bucket, replays
+ * the graph and returns per query min(k[q], found) hits in out[nq][max_k]
+ * ascending by (dist, id); queries whose reduced-precision superset cannot
+ * be certified are re-run exactly on g, and batches whose predicates exceed
+ * the bucket's capacity (8 instructions and 8 IN values per query on
+ * average) run through g's ordinary path. *device_ms: the graph's device
+ * time. g must outlive the stream; calls on one stream are serialized. */
+#define PV_STREAM_MAX_K 256
+typedef struct PvStream PvStream;
+PvStream *pv_stream_create(FvGpuIndex *g, int max_batch, uint32_t max_k,
+                           const float *tune_queries, int ntune, const char *tune_path,
+                           char *errbuf, size_t errlen);
+int pv_stream_run(PvStream *s, int nq, const float *queries, const FvGpuQueryDesc *qd,
+                  const FvGpuPredNode *nodes, int nnodes, const int32_t *children,
+                  int nchildren, const double *invals, int ninvals, const uint32_t *k,
+                  FvHit *out, uint32_t *out_cnt, float *device_ms, char *errbuf,
+                  size_t errlen);
+/* Bucket i's size, width and tuned plan (mode PV_MODE_EXACT / PV_MODE_LOW,
+ * epilogue groups, stages, CTAs along the rows; 0 = built-in) and measured
+ * ms; returns the number of buckets (i < 0: just the number). */
+int pv_stream_info(PvStream *s, int i, int *B, uint32_t *topb, int *mode, int *epi, int *ns,
+                   int *grow, float *tuned_ms);
+/* Queries of the last run re-run exactly; 1 if it bypassed the graphs. */
+int pv_stream_last(PvStream *s, int *uncertain, int *fallback);
+void pv_stream_free(PvStream *s);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 
@@ -259,6 +294,13 @@ float pv_last_kernel_ms(const FvGpuIndex *g);
  * exact FP32 (4 x topb, or topb when its BF16 distances were certified
  * exact: integer rows and queries with all sums below 2^24); 0 if none. */
 int pv_last_superset(const FvGpuIndex *g);
+
+/* Queries of the last reduced-precision batch call on g whose candidate
+ * superset the merge could not certify complete (a per-CTA candidate list
+ * of 64 filled up below the superset's last key). fv_gpu_brute_batch and
+ * pv_routed_batch re-run those queries with the exact scan; pv_batch_fetch
+ * only reports them. */
+int pv_last_uncertain(const FvGpuIndex *g);
 
 /* Kernels launched by the last batch call on g (summed over the iterations
  * of pv_batch_run). */

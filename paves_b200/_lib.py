@@ -102,6 +102,7 @@ _EXT_SIGS = {
     "pv_last_kernel_ms": (C.c_float, [P]),
     "pv_last_superset": (C.c_int, [P]),
     "pv_last_launches": (C.c_int, [P]),
+    "pv_last_uncertain": (C.c_int, [P]),
     "pv_graph_stats": (C.c_int, [P, P, C.c_int]),
 }
 PV_MODE_EXACT, PV_MODE_LOW = 0, 1
@@ -181,3 +182,14 @@ _EXT_SIGS.update({
 _EXT_SIGS["pv_routed_batch"] = (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int,
                                           P, C.c_uint32, P, C.c_float, P, P, P, P, P, C.c_char_p,
                                           C.c_size_t])
+
+PV_STREAM_MAX_K = 256
+_EXT_SIGS.update({
+    "pv_stream_create": (P, [P, C.c_int, C.c_uint32, P, C.c_int, C.c_char_p, C.c_char_p,
+                             C.c_size_t]),
+    "pv_stream_run": (C.c_int, [P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int, P, P, P, P,
+                                C.c_char_p, C.c_size_t]),
+    "pv_stream_info": (C.c_int, [P, C.c_int, P, P, P, P, P, P, P]),
+    "pv_stream_last": (C.c_int, [P, P, P]),
+    "pv_stream_free": (None, [P]),
+})

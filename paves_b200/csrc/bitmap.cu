@@ -100,25 +100,34 @@ bitmap_kernel(const double *__restrict__ cols, uint64_t nrows,
 // All programs of a batch in one pass: a warp takes 4 consecutive 32-row
 // words and evaluates every program on them, 4 rows per lane in flight, so
 // a column's values are fetched from HBM once per batch and re-read from
-// L1 by the other programs. Programs and constants live in shared memory.
-constexpr int BM_MAX_INSNS = 512;
-constexpr int BM_MAX_PROGS = 1024;
-constexpr int BM_MAX_CONSTS = 512;
-
+// L1 by the other programs. Programs and constants live in shared memory
+// (dynamic: up to the launch's capacities). dcounts, if given, holds the
+// batch's {P, ninsns, nconsts} in device memory (each <= its capacity), so
+// one launch shape serves batches of varying predicates.
 __global__ void __launch_bounds__(256)
 bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                     const PredInsn *__restrict__ insns, int ninsns,
                     const PredProg *__restrict__ progs, int P,
                     const double *__restrict__ consts, int nconsts,
+                    const int *__restrict__ dcounts,
                     uint32_t *__restrict__ bitmaps, uint64_t bm_words,
                     unsigned long long *__restrict__ popcnt) {
-    __shared__ PredInsn s_ins[BM_MAX_INSNS];
-    __shared__ PredProg s_prog[BM_MAX_PROGS];
-    __shared__ double s_const[BM_MAX_CONSTS];
-    __shared__ unsigned int s_cnt[BM_MAX_PROGS];
+    extern __shared__ __align__(16) unsigned char bm_smem[];
+    PredInsn *s_ins = (PredInsn *)bm_smem;                    // [ninsns cap]
+    PredProg *s_prog = (PredProg *)(s_ins + ninsns);          // [P cap]
+    double *s_const = (double *)(s_prog + P + (P & 1));       // [nconsts cap]
+    unsigned int *s_cnt = (unsigned int *)(s_const + nconsts);  // [P cap]
+    if (dcounts) {
+        P = min(P, dcounts[0]);
+        ninsns = min(ninsns, dcounts[1]);
+        nconsts = min(nconsts, dcounts[2]);
+    }
     for (int i = threadIdx.x; i < ninsns; i += blockDim.x) s_ins[i] = insns[i];
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        s_prog[i] = progs[i];
+        PredProg pg = progs[i];
+        // a program reaching past the copied instructions evaluates to false
+        if (pg.insn0 < 0 || pg.ninsn < 0 || pg.insn0 + pg.ninsn > ninsns) pg.ninsn = 0;
+        s_prog[i] = pg;
         s_cnt[i] = 0;
     }
     for (int i = threadIdx.x; i < nconsts; i += blockDim.x) s_const[i] = consts[i];
@@ -152,7 +161,10 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                             b = cmp_op(v[j], in.op, in.value);
                         } else {
                             b = false;
-                            for (int k = 0; k < in.n; k++) b |= (v[j] == s_const[in.val0 + k]);
+                            for (int k = 0; k < in.n; k++) {
+                                const int ci = in.val0 + k;
+                                b |= ci < nconsts && v[j] == s_const[ci];
+                            }
                         }
                         st[j] = (st[j] << 1) | (b ? 1u : 0u);
                     }
@@ -188,6 +200,32 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
         if (s_cnt[p]) atomicAdd(popcnt + p, (unsigned long long)s_cnt[p]);
 }
 
+size_t bitmap_multi_smem(int P, int ninsns, int nconsts) {
+    return (size_t)ninsns * sizeof(PredInsn) + (size_t)(P + (P & 1)) * sizeof(PredProg) +
+           (size_t)nconsts * 8 + (size_t)P * 4;
+}
+constexpr size_t BM_SMEM_MAX = 200 * 1024;
+
+static cudaError_t launch_multi(const double *cols, uint64_t nrows, const PredInsn *insns,
+                                const PredProg *progs, const double *consts, int P,
+                                int ninsns, int nconsts, const int *dcounts,
+                                uint32_t *bitmaps, uint64_t bm_words,
+                                unsigned long long *popcnt, int sm_count, cudaStream_t st) {
+    const size_t smem = bitmap_multi_smem(P, ninsns, nconsts);
+    cudaError_t e = cudaFuncSetAttribute(bitmap_multi_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint64_t groups = (bm_words + 3) / 4;
+    uint64_t blocks = (groups + 7) / 8;
+    const uint64_t cap = (uint64_t)sm_count * (smem <= 48 * 1024 ? 4 : 1);
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    bitmap_multi_kernel<<<(unsigned)blocks, 256, smem, st>>>(cols, nrows, insns, ninsns, progs, P,
+                                                             consts, nconsts, dcounts, bitmaps,
+                                                             bm_words, popcnt);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words,
@@ -196,17 +234,9 @@ cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *i
     if (P <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(popcnt, 0, sizeof(unsigned long long) * P, st);
     if (e != cudaSuccess) return e;
-    if (ninsns <= BM_MAX_INSNS && P <= BM_MAX_PROGS && nconsts <= BM_MAX_CONSTS) {
-        const uint64_t groups = (bm_words + 3) / 4;
-        uint64_t blocks = (groups + 7) / 8;
-        const uint64_t cap = (uint64_t)sm_count * 4;
-        if (blocks > cap) blocks = cap;
-        if (blocks == 0) blocks = 1;
-        bitmap_multi_kernel<<<(unsigned)blocks, 256, 0, st>>>(cols, nrows, insns, ninsns, progs,
-                                                              P, consts, nconsts, bitmaps,
-                                                              bm_words, popcnt);
-        return cudaGetLastError();
-    }
+    if (bitmap_multi_smem(P, ninsns, nconsts) <= BM_SMEM_MAX)
+        return launch_multi(cols, nrows, insns, progs, consts, P, ninsns, nconsts, nullptr,
+                            bitmaps, bm_words, popcnt, sm_count, st);
     uint64_t blocks = (bm_words + 7) / 8;
     uint64_t cap = (uint64_t)sm_count * 8;
     if (blocks > cap) blocks = cap;
@@ -215,6 +245,19 @@ cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *i
     bitmap_kernel<<<grid, 256, 0, st>>>(cols, nrows, insns, progs, consts, bitmaps,
                                         bm_words, popcnt);
     return cudaGetLastError();
+}
+
+cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const PredInsn *insns,
+                                  const PredProg *progs, const double *consts,
+                                  const int *dcounts, int P_cap, int insn_cap, int const_cap,
+                                  uint32_t *bitmaps, uint64_t bm_words,
+                                  unsigned long long *popcnt, int sm_count, cudaStream_t st) {
+    if (P_cap <= 0) return cudaSuccess;
+    if (bitmap_multi_smem(P_cap, insn_cap, const_cap) > BM_SMEM_MAX) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(popcnt, 0, sizeof(unsigned long long) * P_cap, st);
+    if (e != cudaSuccess) return e;
+    return launch_multi(cols, nrows, insns, progs, consts, P_cap, insn_cap, const_cap, dcounts,
+                        bitmaps, bm_words, popcnt, sm_count, st);
 }
 
 }  // namespace pv

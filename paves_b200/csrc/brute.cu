@@ -17,6 +17,7 @@
 #include <algorithm>
 
 #include "index.h"
+#include "paves_ext.h"
 #include "pv_internal.h"
 
 namespace pv {
@@ -83,6 +84,16 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     if (ev) cudaEventRecord(ev[0], g->stream);
     if (bitmaps_ready) {
         // the caller launched the bitmaps of this batch
+    } else if (db.counts_on_device && P > 0) {
+        PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
+        PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
+        g->launches++;
+        PV_CUDA_OK(launch_bitmaps_capped(g->d_cols, g->count, d_insns, d_progs, d_consts,
+                                         (const int *)(d + db.off_counts), P, db.ninsns,
+                                         db.nconsts, s.bitmaps.as<uint32_t>(), bm_words,
+                                         s.popcnt.as<unsigned long long>(), g->sm_count,
+                                         g->stream),
+                   errbuf, errlen);
     } else if (P > 0) {
         PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
         PV_CUDA_OK(s.popcnt.ensure((size_t)P * 8), errbuf, errlen);
@@ -104,6 +115,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         return 0;
     }
     g->tc_err = nullptr;
+    g->tc_unc = nullptr;
 
     ScanPlan pl;
     if (!plan_scan_f32(g->count, g->dpad, nq, (int)topb, g->sm_count, pl)) {
@@ -188,6 +200,61 @@ extern "C" int fv_gpu_brute_batch(FvGpuIndex *g, int nq, const float *queries,
 
 namespace pv {
 
+// Re-runs exactly the queries whose reduced-precision superset the last TC
+// merge could not certify (a full per-CTA list may have dropped a member of
+// it) and writes their results over the caller's out / out_cnt / truncated
+// (stride topb). Call after the batch's results were copied out: the re-run
+// reuses the index's staging buffers.
+int tc_redo_uncertain(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                      uint32_t topb, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
+                      char *errbuf, size_t errlen) {
+    g->last_uncertain = 0;
+    if (!g->tc_unc) return 0;
+    std::vector<uint8_t> unc((size_t)nq);
+    PV_CUDA_OK(cudaMemcpyAsync(unc.data(), g->tc_unc, (size_t)nq, cudaMemcpyDeviceToHost,
+                               g->stream),
+               errbuf, errlen);
+    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    g->tc_unc = nullptr;
+    return redo_flagged(g, nq, queries, pb, topb, unc.data(), out, out_cnt, truncated, errbuf,
+                        errlen);
+}
+
+int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                 uint32_t topb, const uint8_t *unc, FvHit *out, uint32_t *out_cnt,
+                 uint8_t *truncated, char *errbuf, size_t errlen) {
+    g->last_uncertain = 0;
+    std::vector<int> idx;
+    for (int q = 0; q < nq; q++)
+        if (unc[q]) idx.push_back(q);
+    g->last_uncertain = (int)idx.size();
+    if (idx.empty()) return 0;
+    const int n = (int)idx.size(), dim = g->dim;
+    std::vector<float> sq((size_t)n * dim);
+    PredBatch sub = pb;
+    for (int i = 0; i < n; i++) {
+        memcpy(&sq[(size_t)i * dim], queries + (size_t)idx[i] * dim, sizeof(float) * dim);
+        sub.qprog[i] = pb.qprog[idx[i]];
+    }
+    sub.qprog.resize(n);
+    std::vector<FvHit> so((size_t)n * topb);
+    std::vector<uint32_t> sc(n);
+    std::vector<uint8_t> st(n);
+    const int launches = g->launches, nunc = n;
+    if (brute_run_host(g, n, sq.data(), sub, topb, PV_MODE_EXACT, so.data(), sc.data(),
+                       st.data(), errbuf, errlen))
+        return -1;
+    g->launches += launches;
+    g->last_uncertain = nunc;
+    for (int i = 0; i < n; i++) {
+        const int q = idx[i];
+        memcpy(out + (size_t)q * topb, &so[(size_t)i * topb], sizeof(FvHit) * sc[i]);
+        out_cnt[q] = sc[i];
+        truncated[q] = st[i];
+    }
+    return 0;
+}
+
 int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
                    uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
                    char *errbuf, size_t errlen) {
@@ -222,7 +289,7 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
         out_cnt[q] = c;
     }
     memcpy(truncated, oh + off_tr, (size_t)nq);
-    return 0;
+    return tc_redo_uncertain(g, nq, queries, pb, topb, out, out_cnt, truncated, errbuf, errlen);
 }
 
 }  // namespace pv

@@ -143,8 +143,18 @@ extern "C" int pv_batch_fetch(PvBatch *b, FvHit *out, uint32_t *out_cnt, uint8_t
         out_cnt[q] = c;
     }
     memcpy(truncated, oh + b->off_tr, (size_t)nq);
+    // prepared batches report, and do not re-run, uncertified supersets
+    g->last_uncertain = 0;
+    if (g->tc_unc && g->tc_unc_n == nq) {
+        std::vector<uint8_t> unc((size_t)nq);
+        PV_CUDA_OK(cudaMemcpy(unc.data(), g->tc_unc, (size_t)nq, cudaMemcpyDeviceToHost), errbuf,
+                   errlen);
+        for (int q = 0; q < nq; q++) g->last_uncertain += unc[q] ? 1 : 0;
+    }
     return 0;
 }
+
+extern "C" int pv_last_uncertain(const FvGpuIndex *g) { return g ? g->last_uncertain : 0; }
 
 extern "C" void pv_batch_free(PvBatch *b) {
     if (!b) return;

@@ -167,14 +167,16 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
     if (!g) return;
     if (g->device >= 0) cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
-    cudaFree(g->d_vecs);
-    cudaFree(g->d_cols);
-    cudaFree(g->d_prows);
-    cudaFree(g->d_adj);
-    cudaFree(g->d_deg);
-    cudaFree(g->d_vlow);
-    cudaFree(g->d_vscale);
-    cudaFree(g->d_norm);
+    if (!g->view) {  // a view borrows the device data of its parent
+        cudaFree(g->d_vecs);
+        cudaFree(g->d_cols);
+        cudaFree(g->d_prows);
+        cudaFree(g->d_adj);
+        cudaFree(g->d_deg);
+        cudaFree(g->d_vlow);
+        cudaFree(g->d_vscale);
+        cudaFree(g->d_norm);
+    }
     Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
                    &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
                    &g->scan.out_d, &g->scan.out_h, &g->graph.visited, &g->graph.res,
@@ -321,3 +323,43 @@ extern "C" int fv_gpu_mem_probe(uint64_t *free_bytes, uint64_t *total_bytes) {
     if (total_bytes) *total_bytes = t;
     return probed;
 }
+
+namespace pv {
+
+// A handle that shares g's device data and owns its own stream, events and
+// scratch: work captured into CUDA graphs on the view keeps fixed scratch
+// addresses whatever other calls do on g. Freed with fv_gpu_index_free
+// (scratch only); must not outlive g.
+FvGpuIndex *index_view(const FvGpuIndex *g) {
+    FvGpuIndex *v = new FvGpuIndex();
+    v->device = g->device;
+    v->precision = g->precision;
+    v->count = g->count;
+    v->dim = g->dim;
+    v->ncols = g->ncols;
+    v->l0_stride = g->l0_stride;
+    v->dpad = g->dpad;
+    v->d_vecs = g->d_vecs;
+    v->d_cols = g->d_cols;
+    v->d_prows = g->d_prows;
+    v->d_adj = g->d_adj;
+    v->d_deg = g->d_deg;
+    v->deg_cap = g->deg_cap;
+    v->kpad = g->kpad;
+    v->d_vlow = g->d_vlow;
+    v->d_vscale = g->d_vscale;
+    v->d_norm = g->d_norm;
+    v->row_amax = g->row_amax;
+    v->sm_count = g->sm_count;
+    v->view = true;
+    if (cudaSetDevice(v->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete v;
+        return nullptr;
+    }
+    cudaEventCreate(&v->ev0);
+    cudaEventCreate(&v->ev1);
+    return v;
+}
+
+}  // namespace pv

@@ -8,6 +8,8 @@ bool pv_bf16_exact(int dim, float row_amax, float q_amax);
 
 namespace pv {
 
+FvGpuIndex *index_view(const FvGpuIndex *g);  // index.cu
+
 // ---- predicates (pred.cpp, bitmap.cu)
 int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
                        const FvGpuPredNode *nodes, int nnodes, const int32_t *children,
@@ -17,6 +19,14 @@ cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *i
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words, unsigned long long *popcnt,
                            int sm_count, cudaStream_t st, int ninsns, int nconsts);
+// Same, with the batch's {P, ninsns, nconsts} read on the device from
+// dcounts (each at most its cap): one launch shape for a CUDA graph.
+size_t bitmap_multi_smem(int P, int ninsns, int nconsts);
+cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const PredInsn *insns,
+                                  const PredProg *progs, const double *consts,
+                                  const int *dcounts, int P_cap, int insn_cap, int const_cap,
+                                  uint32_t *bitmaps, uint64_t bm_words,
+                                  unsigned long long *popcnt, int sm_count, cudaStream_t st);
 
 // ---- exact FP32 scan (scan_f32.cu)
 struct ScanF32Args {
@@ -53,7 +63,8 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          const int32_t *qprog, const unsigned long long *popcnt,
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
                          uint8_t *trunc, cudaStream_t st,
-                         unsigned long long *tau_out = nullptr);
+                         unsigned long long *tau_out = nullptr, int kout = 0,
+                         uint8_t *unc = nullptr);
 
 // ---- batch staging (brute.cu)
 struct DevBatch {
@@ -63,6 +74,10 @@ struct DevBatch {
     size_t off_q = 0, off_qprog = 0, off_progs = 0, off_insns = 0, off_consts = 0, off_extra = 0;
     size_t bytes = 0;
     float q_amax = -1.f;  // max |q| if all queries are integers <= 256, else -1
+    // {P, ninsns, nconsts} also staged at off_counts: P / ninsns / nconsts
+    // above are then capacities and the bitmap kernel reads the counts
+    bool counts_on_device = false;
+    size_t off_counts = 0;
 };
 
 int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
@@ -74,11 +89,20 @@ int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen);
 int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
                  uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
                  cudaEvent_t *ev = nullptr, bool bitmaps_ready = false);
+// Re-runs exactly the queries with unc[q] != 0 on g (host buffers; call with
+// g->mu held) and writes their results over out / out_cnt / truncated.
+int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                 uint32_t topb, const uint8_t *unc, FvHit *out, uint32_t *out_cnt,
+                 uint8_t *truncated, char *errbuf, size_t errlen);
+int tc_redo_uncertain(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+                      uint32_t topb, FvHit *out, uint32_t *out_cnt, uint8_t *truncated,
+                      char *errbuf, size_t errlen);
 int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
                    uint32_t topb, int mode, FvHit *out, uint32_t *out_cnt,
                    uint8_t *truncated, char *errbuf, size_t errlen);
 
 // ---- tensor-core scan (scan_tc.cu)
+bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns);
 int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax);
 bool tc_supported(const FvGpuIndex *g);
 int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,

@@ -936,6 +936,11 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
             memcpy(out + (size_t)q * topb, oh + (size_t)q * topb * sizeof(FvHit), c * sizeof(FvHit));
             out_cnt[q] = c;
         }
+        std::vector<uint8_t> tr(nq);
+        if (tc_redo_uncertain(g, nq, queries, pb, topb, out, out_cnt, tr.data(), errbuf, errlen))
+            return -1;
+        for (int q = 0; q < nq; q++)
+            if (out_cnt[q] > k[q]) out_cnt[q] = k[q];
     }
     float t[3] = {0, 0, 0};
     cudaEventElapsedTime(&t[0], ev[0], ev[1]);

@@ -207,7 +207,8 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
              const int32_t *__restrict__ qprog,
              const unsigned long long *__restrict__ popcnt, uint64_t nrows,
              FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
-             uint8_t *__restrict__ trunc, unsigned long long *__restrict__ tau_out) {
+             uint8_t *__restrict__ trunc, unsigned long long *__restrict__ tau_out,
+             int KO, uint8_t *__restrict__ unc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *buf = (uint64_t *)smem_raw;   // [M]
     int *s_c = (int *)(buf + M);            // [grow] prefix lengths
@@ -261,8 +262,8 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
                 __syncthreads();
             }
         }
-        const int nt = nfast < K ? nfast : K;
-        for (int i = nt + tid; i < K; i += blockDim.x) buf[i] = KEY_MAX;
+        const int nt = nfast < KO ? nfast : KO;
+        for (int i = nt + tid; i < KO; i += blockDim.x) buf[i] = KEY_MAX;
         __syncthreads();
     } else {
     // general path: measure each list's prefix, then fold in rounds
@@ -338,33 +339,47 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
             }
         }
         __syncthreads();
-        nt = n < K ? n : K;
+        nt = n < KO ? n : KO;
         g = gend;
     }
-    for (int i = nt + tid; i < K; i += blockDim.x) buf[i] = KEY_MAX;
+    for (int i = nt + tid; i < KO; i += blockDim.x) buf[i] = KEY_MAX;
     __syncthreads();
     }  // general path
-    for (int i = tid; i < K; i += blockDim.x) {
+    for (int i = tid; i < KO; i += blockDim.x) {
         const uint64_t k = buf[i];
         if (k != KEY_MAX) {
             FvHit h;
             h.node = (uint64_t)key_row(k);
             h.dist = key_dist(k);
-            out[(uint64_t)q * K + i] = h;
+            out[(uint64_t)q * KO + i] = h;
         }
     }
+    __shared__ int s_lo, s_unc;
     if (tid == 0) {
-        int lo = 0, hi = K;
+        int lo = 0, hi = KO;
         while (lo < hi) {
             int mid = (lo + hi) >> 1;
             if (buf[mid] != KEY_MAX) lo = mid + 1; else hi = mid;
         }
+        s_lo = lo;
+        s_unc = 0;
         out_cnt[q] = (uint32_t)lo;
         const int pg = qprog[q];
         const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
-        trunc[q] = passing > (unsigned long long)K ? 1 : 0;
-        // the K-th merged key bounds the K-th key of any superset of rows
-        if (tau_out && lo == K) tau_out[q] = buf[K - 1];
+        trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
+        // the KO-th merged key bounds the KO-th key of any superset of rows
+        if (tau_out && lo == KO) tau_out[q] = buf[KO - 1];
+    }
+    if (unc) {
+        // Lists shorter than the output: a full list whose last key is at
+        // or below the output's last key (or below the bound while the
+        // output is short) may have dropped a member of it.
+        __syncthreads();
+        const uint64_t lim = s_lo == KO ? buf[KO - 1] : bound;
+        for (int g = tid; g < grow; g += blockDim.x)
+            if (cnts[g] >= (uint32_t)K && lists[(uint64_t)g * K + K - 1] <= lim) s_unc = 1;
+        __syncthreads();
+        if (tid == 0) unc[q] = (uint8_t)s_unc;
     }
 }
 
@@ -466,12 +481,16 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          const ScanPlan &pl, const unsigned long long *tau,
                          const int32_t *qprog, const unsigned long long *popcnt,
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
-                         uint8_t *trunc, cudaStream_t st, unsigned long long *tau_out) {
+                         uint8_t *trunc, cudaStream_t st, unsigned long long *tau_out,
+                         int kout, uint8_t *unc) {
+    if (kout <= 0) kout = K;
+    if (kout > pl.M) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)pl.merge_smem);
     if (e != cudaSuccess) return e;
     merge_kernel<<<nq, 256, pl.merge_smem, st>>>(part, part_cnt, grow, K, pl.M, tau, qprog,
-                                                 popcnt, nrows, out, out_cnt, trunc, tau_out);
+                                                 popcnt, nrows, out, out_cnt, trunc, tau_out,
+                                                 kout, unc);
     return cudaGetLastError();
 }
 

@@ -41,6 +41,13 @@ constexpr int TC_BN = 128;          // rows per tile (MMA N)
 constexpr int TC_KB_BYTES = 128;    // bytes of K per swizzle row / TMA box
 constexpr int TC_BOX = TC_BN * TC_KB_BYTES;  // 16 KB per K-block box
 constexpr int TC_KBS = 2;           // K-blocks per pipeline stage
+// Candidates per query kept for the exact re-rank at most (the superset),
+// and the list length per (query, CTA half) that holds them: when the
+// superset is longer than a list, the union of the lists is the superset
+// only if no full list could have dropped a member of it, which the merge
+// certifies per query (queries it cannot certify are re-run exactly).
+constexpr int TC_MAX_SUPERSET = 1024;
+constexpr int TC_MAX_LIST = 64;
 
 template <bool FP8>
 __device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
@@ -58,7 +65,8 @@ struct TcArgs {
     uint64_t tiles_per_cta;
     uint64_t tile0_mul;  // first tile of CTA group g = g * tile0_mul
     uint64_t tile_step;  // stride between a CTA's tiles
-    int KP;             // candidates kept per query (K')
+    int KP;             // list length per (query, CTA half)
+    int push_tau;       // a full list's last key bounds the superset (lists hold it all)
     int NS;             // pipeline stages
     const float *__restrict__ xnorm;   // [rows padded to 128]
     const float *__restrict__ xscale;  // fp8: per-row scale, else null
@@ -342,7 +350,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             tc_fence_before();
             mbar_arrive(&tempty[acc]);
             if (tr) a.trace[t * 4 + 3] = globaltimer();
-            if (qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
+            if (a.push_tau && qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
 #pragma unroll
             for (int j = 0; j < CPH; j++) {
                 xr[j] = nxr[j];
@@ -423,54 +431,70 @@ __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad,
 }
 
 // ---------------------------------------------------------------- re-rank
-// Exact FP32 distances (difference form) for each query's K' merged
-// candidates; keeps the best topb by (dist, id). One CTA (4 warps) per query.
-__global__ void __launch_bounds__(128)
+// Exact FP32 distances (difference form) for each query's merged candidates
+// (up to TC_MAX_SUPERSET, row stride S); keeps the best topb by (dist, id).
+// One CTA (8 warps) per query: 8 lanes per candidate, 32 candidates in
+// flight, then a bitonic sort of the keys in shared memory.
+__global__ void __launch_bounds__(256)
 rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict__ queries,
-              const FvHit *__restrict__ cand, const uint32_t *__restrict__ cand_cnt, int KP,
+              const FvHit *__restrict__ cand, const uint32_t *__restrict__ cand_cnt, int S,
               uint32_t topb, const int32_t *__restrict__ qprog,
               const unsigned long long *__restrict__ popcnt, uint64_t nrows,
               FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
               uint8_t *__restrict__ trunc) {
-    __shared__ uint64_t keys[64];
-    const int q = blockIdx.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ uint64_t keys[TC_MAX_SUPERSET];
+    const int q = blockIdx.x, tid = threadIdx.x;
+    const int grp = tid >> 3, sub = tid & 7;
     int n = (int)cand_cnt[q];
-    if (n > KP) n = KP;
+    if (n > S) n = S;
     const float *qv = queries + (size_t)q * dpad;
-    for (int j = warp; j < n; j += 4) {
-        const uint32_t row = (uint32_t)cand[(size_t)q * KP + j].node;
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + grp;
+        const bool ok = j < n;
+        const uint32_t row = (uint32_t)cand[(size_t)q * S + (ok ? j : 0)].node;
         const float *x = vecs + (size_t)row * dpad;
         float acc = 0.f;
-        for (int k = lane * 4; k < dpad; k += 128) {
-            float4 v = __ldg((const float4 *)(x + k));
-            float4 w = __ldg((const float4 *)(qv + k));
-            float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
+        for (int k = sub * 4; k < dpad; k += 32) {
+            const float4 v = __ldg((const float4 *)(x + k));
+            const float4 w = __ldg((const float4 *)(qv + k));
+            const float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
             acc = fmaf(d0, d0, acc);
             acc = fmaf(d1, d1, acc);
             acc = fmaf(d2, d2, acc);
             acc = fmaf(d3, d3, acc);
         }
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) keys[j] = make_key(acc, row);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        if (ok && sub == 0) keys[j] = make_key(acc, row);
     }
+    int n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (int i = n + tid; i < n2; i += blockDim.x) keys[i] = KEY_MAX;
     __syncthreads();
-    // rank placement (keys are unique): position = number of smaller keys
-    uint64_t mine = 0;
-    int rank = 0;
-    if ((int)threadIdx.x < n) {
-        mine = keys[threadIdx.x];
-        for (int j = 0; j < n; j++) rank += keys[j] < mine;
+    for (int k = 2; k <= n2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < (n2 >> 1); i += blockDim.x) {
+                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                const int hi = lo | j;
+                const uint64_t x = keys[lo], y = keys[hi];
+                if ((x > y) == ((lo & k) == 0)) {
+                    keys[lo] = y;
+                    keys[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
     }
-    __syncthreads();
-    if ((int)threadIdx.x < n && rank < (int)topb) {
+    const int nout = n < (int)topb ? n : (int)topb;
+    for (int i = tid; i < nout; i += blockDim.x) {
         FvHit h;
-        h.node = key_row(mine);
-        h.dist = key_dist(mine);
-        out[(size_t)q * topb + rank] = h;
+        h.node = key_row(keys[i]);
+        h.dist = key_dist(keys[i]);
+        out[(size_t)q * topb + i] = h;
     }
-    if (threadIdx.x == 0) {
-        out_cnt[q] = (uint32_t)(n < (int)topb ? n : (int)topb);
+    if (tid == 0) {
+        out_cnt[q] = (uint32_t)nout;
         const int pg = qprog[q];
         const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
         trunc[q] = passing > (unsigned long long)topb ? 1 : 0;
@@ -508,17 +532,16 @@ static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner,
     return r == CUDA_SUCCESS;
 }
 
-// Candidates kept per query before the exact re-rank: 4k while the scan's
-// distances may be inexact; k itself when the upload certified that BF16
-// distances are exact (integer rows, |x| <= 256, all sums below 2^24), since
-// then the scan's top-k already is the exact top-k. 0 = topb too large.
+// Candidates kept per query before the exact re-rank (the superset): 4k
+// while the scan's distances may be inexact; k itself when the upload
+// certified that BF16 distances are exact (integer rows, |x| <= 256, all
+// sums below 2^24), since then the scan's top-k already is the exact top-k.
+// 0 = topb too large.
 int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax) {
     const bool exact =
         g->precision != FV_GPU_PREC_FP8 && pv_bf16_exact(g->dim, g->row_amax, q_amax);
-    int kp = exact ? (int)topb : 4 * (int)topb;
-    if (kp > 64) kp = 64;
-    if (kp < (int)topb) return 0;  // topb beyond the superset capacity
-    return kp;
+    const int s = exact ? (int)topb : 4 * (int)topb;
+    return s <= TC_MAX_SUPERSET ? s : 0;  // 0: topb beyond the superset capacity
 }
 
 bool tc_supported(const FvGpuIndex *g) {
@@ -531,6 +554,15 @@ static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
     return 1024 + (size_t)kblocks * TC_BOX + (size_t)NS * TC_KBS * TC_BOX +
            (size_t)TC_BM * EPI * KP * 8 + (size_t)32 * TC_BM * EPI * 4 +
            (size_t)(2 * NS + 6) * 8;
+}
+
+bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
+    if (!tc_supported(g) || (epi != 1 && epi != 2) || ns < 2 || ns > 4) return false;
+    const int S = tc_superset(g, topb, -1.f);
+    if (!S) return false;
+    const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
+    const int esz = g->precision == FV_GPU_PREC_FP8 ? 1 : 2;
+    return tc_smem(g->kpad * esz / TC_KB_BYTES, ns, KP, epi) <= 227 * 1024;
 }
 
 template <int EPI>
@@ -559,9 +591,11 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const bool fp8 = g->precision == FV_GPU_PREC_FP8;
     const int esz = fp8 ? 1 : 2;
     const int kblocks = g->kpad * esz / TC_KB_BYTES;
-    const int KP = tc_superset(g, topb, q_amax);
-    g->last_superset = KP;
-    if (!KP || !tc_supported(g)) {
+    const int S = tc_superset(g, topb, q_amax);
+    const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
+    g->last_superset = S;
+    g->tc_unc = nullptr;
+    if (!S || !tc_supported(g)) {
         snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
         return -1;
     }
@@ -575,11 +609,18 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         NS = 4;
         while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
     }
+    if (g->tune_epi || g->tune_ns) {  // a tuned shape, if it fits
+        const int e = g->tune_epi ? g->tune_epi : EPI, n = g->tune_ns ? g->tune_ns : NS;
+        if ((e == 1 || e == 2) && n >= 2 && n <= 4 && tc_smem(kblocks, n, KP, e) <= smem_cap) {
+            EPI = e;
+            NS = n;
+        }
+    }
     const size_t smem = tc_smem(kblocks, NS, KP, EPI);
     const int qtiles = (nq + TC_BM - 1) / TC_BM;
     const int nqpad = qtiles * TC_BM;
     const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;
-    int grow = g->sm_count / qtiles;
+    int grow = g->tune_grow > 0 ? g->tune_grow : g->sm_count / qtiles;
     if (grow < 1) grow = 1;
     uint64_t maxg = (ntiles_all + 3) / 4;
     if ((uint64_t)grow > maxg) grow = (int)maxg;
@@ -592,9 +633,10 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const size_t off_qs = off_qn + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
     const size_t off_err = off_qs + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
     const size_t off_cand = off_err + 256;
-    const size_t off_ccnt = off_cand + (((size_t)nq * KP * sizeof(FvHit) + 255) & ~(size_t)255);
+    const size_t off_ccnt = off_cand + (((size_t)nq * S * sizeof(FvHit) + 255) & ~(size_t)255);
     const size_t off_ctr = off_ccnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
-    const size_t cbytes = off_ctr + (size_t)nq + 256;
+    const size_t off_unc = off_ctr + (((size_t)nq + 255) & ~(size_t)255);
+    const size_t cbytes = off_unc + (size_t)nq + 256;
     PV_CUDA_OK(s.cand.ensure(cbytes), errbuf, errlen);
     PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
     const int nlists = grow * EPI;  // partial lists per query
@@ -625,6 +667,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.grow = grow;
     a.tiles_per_cta = tpc;
     a.KP = KP;
+    a.push_tau = KP == S ? 1 : 0;
     a.NS = NS;
     a.xnorm = g->d_norm;
     a.xscale = fp8 ? g->d_vscale : nullptr;
@@ -671,7 +714,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sp.merge_smem = (size_t)sp.M * 8 + (size_t)nlists * 8;
         PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, sp, a.tau, d_qprog, popcnt,
                                 g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
-                                a.tau),
+                                a.tau, S),
                    errbuf, errlen);
     }
     // stage boundary: everything before the main pass (bitmaps, query prep,
@@ -684,10 +727,14 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     ScanPlan pl;
     pl.M = 4096;
     pl.merge_smem = (size_t)pl.M * 8 + (size_t)nlists * 8;
+    uint8_t *d_unc = KP < S ? (uint8_t *)(c + off_unc) : nullptr;
     PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, pl, a.tau, d_qprog, popcnt, g->count,
-                            nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream),
+                            nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream, nullptr, S,
+                            d_unc),
                errbuf, errlen);
-    rerank_kernel<<<nq, 128, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, KP, topb,
+    g->tc_unc = d_unc;
+    g->tc_unc_n = nq;
+    rerank_kernel<<<nq, 256, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, S, topb,
                                              d_qprog, popcnt, g->count, d_out, d_cnt, d_trunc);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
     if (ev) cudaEventRecord(ev[3], g->stream);

@@ -101,3 +101,37 @@ def test_large_topb_falls_back_to_exact(bf16_golden, brute_golden):
     ids, dists, cnt, _ = bf16_golden.brute_batch(g["queries"], [None] * nq, 100)
     for q in range(nq):
         assert np.array_equal(ids[q].astype(np.int64), g["ids100"][0, q])
+
+
+@pytest.mark.parametrize("clustered", [False, True])
+def test_fp8_large_k_superset_certified_or_rerun(clustered):
+    """k = 100 on FP8 keeps a 400-candidate superset from per-CTA lists of
+    64; queries whose superset cannot be certified are re-run exactly. With
+    rows stored cluster by cluster, a query's nearest rows crowd a few lists,
+    so most queries take the exact re-run."""
+    from paves_b200 import _lib
+    ds = datagen.make_dataset(20000, 96, nq=32, ncomp=64)
+    vecs, cols = ds.vectors, ds.cols
+    if clustered:
+        order = np.argsort(((vecs[:, None, :8] - ds.centers[None, :, :8]) ** 2).sum(2).argmin(1),
+                           kind="stable")
+        vecs, cols = np.ascontiguousarray(vecs[order]), np.ascontiguousarray(cols[:, order])
+    gi = GpuIndex(vecs, cols, precision=FV_GPU_PREC_FP8)
+    preds = [None, datagen.six_predicates()["sel70%"]] * 16
+    bp = pred.concat(preds, 20000)
+    ids, dists, cnt, _ = gi.brute_batch_raw(ds.queries, bp, 100)
+    unc = _lib.lib().pv_last_uncertain(gi.handle)
+    assert _lib.lib().pv_last_superset(gi.handle) == 400
+    o_ids, _, _, o_cnt, _ = cpu.exact_topk(vecs, cols, ds.queries, bp, 100)
+    r = recall(ids.astype(np.int64), o_ids.astype(np.int64), o_cnt, 100)
+    assert r >= 0.99, (r, unc)
+    if clustered:
+        assert unc > 0
+    for q in range(32):
+        c = int(cnt[q])
+        assert c == int(o_cnt[q])
+        rows = ids[q, :c].astype(np.int64)
+        exact = np.sum((vecs[rows] - ds.queries[q]) ** 2, 1, dtype=np.float32)
+        assert np.array_equal(dists[q, :c], exact)
+        assert np.all(np.diff(dists[q, :c]) >= 0)
+    gi.close()
