@@ -250,6 +250,111 @@ def kernel_case(name, iters):
     gi.close()
 
 
+def stream_filter(rng):
+    """A per-query filter of selectivity log-uniform in 0.05%..90%: a price
+    range, AND a category set (5 of 10) for a third of the queries."""
+    P, Cc = datagen.COL_PRICE, datagen.COL_CATEGORY
+    sel = float(np.exp(rng.uniform(np.log(0.0005), np.log(0.9))))
+    cat = rng.random() < 1 / 3
+    width = 1000.0 * min(1.0, sel * (2.0 if cat else 1.0))
+    a = float(rng.uniform(0, 1000.0 - width))
+    p = pred.And(pred.Cmp(P, ">=", a), pred.Cmp(P, "<", a + width))
+    if cat:
+        p = pred.And(p, pred.In(Cc, [float(c) for c in sorted(rng.choice(10, 5, replace=False))]))
+    return p
+
+
+def stream_bench(args):
+    """Uneven micro-batches: N = 10M x 96 (256-component mixture), FP8
+    per-row-scaled tensor-core scan + exact FP32 re-rank, sizes log-uniform
+    in 1..512, k from {1, 10, 100} and a filter per query, through the
+    stream's autotuned CUDA graphs (paves_b200.stream). One micro-batch per
+    step; latency = host wall time of the call."""
+    from paves_b200.stream import Stream
+    n, d = 10_000_000, 96
+    ds = datagen.make_dataset(n, d, nq=1024, ncomp=256)
+    gi = GpuIndex(ds.vectors, ds.cols, precision=_lib.FV_GPU_PREC_FP8)
+    tune = os.path.join(tempfile.gettempdir(), f"paves_stream_tune_{n}x{d}.txt")
+    t0 = time.perf_counter()
+    s = Stream(gi, 512, 100, ds.queries[:512], tune)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(datagen.SEED + 9)
+
+    def batch():
+        nq = int(np.clip(np.exp(rng.uniform(0, np.log(512))), 1, 512))
+        idx = rng.integers(0, ds.queries.shape[0], nq)
+        k = rng.choice(np.array([1, 10, 100], np.uint32), nq)
+        return ds.queries[idx], [stream_filter(rng) for _ in range(nq)], k
+
+    for _ in range(max(3, args.warmup)):
+        s.run(*batch())
+    lat, dev, nqs, recs = [], [], [], []
+    clk = Clocks(0)
+    for i in range(args.steps):
+        q, preds, k = batch()
+        t = time.perf_counter()
+        ids, _, cnt, ms = s.run(q, preds, k)
+        lat.append((time.perf_counter() - t) * 1e3)
+        dev.append(ms)
+        nqs.append(len(q))
+        if i % 10 == 0:  # recall against the exact FP32 scan of the same batch
+            bp = pred.concat(preds, n)
+            bx = prepared_batch(gi, q, bp, 100, _lib.PV_MODE_EXACT)
+            batch_run(bx, 1)
+            xi, _, xc, _ = fetch(bx, len(q), 100)
+            _lib.lib().pv_batch_free(bx)
+            for j in range(len(q)):
+                t_ids = xi[j, :min(int(k[j]), int(xc[j]))]
+                if len(t_ids):
+                    recs.append(np.isin(t_ids, ids[j, :cnt[j]]).mean())
+    clocks = clk.stop()
+    lat = np.asarray(lat)
+    line = {
+        "metric": "uneven micro-batch QPS, 10M x 96 L2, FP8 + FP32 re-rank",
+        "value": round(sum(nqs) / (sum(dev) / 1e3), 1), "unit": "queries/s", "n_gpus": 1,
+        "steps": args.steps, "higher_is_better": True, "dtype": "fp8-e4m3", "data": "synthetic",
+        "config": {"workload": "10M x 96 Gaussian-mixture rows (256 components); micro-batch "
+                               "sizes log-uniform 1..512; k in {1, 10, 100} and a filter "
+                               "(selectivity log-uniform 0.05%-90%) per query",
+                   "rows": n, "dim": d, "max_batch": 512, "max_k": 100},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                       "p99": round(float(np.percentile(lat, 99)), 3),
+                       "mean": round(float(lat.mean()), 3)},
+        "device_ms": {"p50": round(float(np.percentile(dev, 50)), 3),
+                      "p99": round(float(np.percentile(dev, 99)), 3)},
+        "e2e": {"value": round(sum(nqs) / (lat.sum() / 1e3), 1), "unit": "queries/s"},
+        "recall_vs_exact": round(float(np.mean(recs)), 4) if recs else None,
+        "queries": int(sum(nqs)), "setup_s": round(setup_s, 1), "plans": s.plans(),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    s.close()
+    gi.close()
+
+
+def shared_graph(vectors, rank, dist, cache):
+    """Rank 0 builds the HNSW graph (or reloads this host's cached copy);
+    after a barrier the other ranks load rank 0's copy instead of building
+    their own."""
+    from paves_b200.hnsw import build_or_load
+    h = build_or_load(vectors, cache, 16, 200) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        h = build_or_load(vectors, cache, 16, 200)
+    return h
+
+
+def reduce_max(vals, dist, device):
+    """Element-wise max over ranks (the job's time is its slowest rank's)."""
+    if not dist:
+        return list(vals)
+    import torch
+    t = torch.tensor(vals, device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -257,9 +362,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="headline", choices=["headline", "stream"],
+                    help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency)")
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES),
                     help="run one batch shape --steps times and exit (for profilers)")
     args = ap.parse_args()
+    if args.workload == "stream":
+        stream_bench(args)
+        return
     if args.kernel_case:
         kernel_case(args.kernel_case, max(1, args.steps))
         return
@@ -287,17 +397,9 @@ def main():
     ds, classes, preds_all = make_workload()
     nclass = len(classes)
     from paves_b200.router import Router, routed_batch
-    from paves_b200.hnsw import build_or_load
-    # rank 0 builds the graph (or reloads this host's cached copy); the
-    # other ranks then load rank 0's copy instead of building their own
     cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
     t_build = time.perf_counter()
-    if rank == 0:
-        hnsw = build_or_load(ds.vectors, cache, 16, 200)
-    if dist:
-        dist.barrier()
-    if rank != 0:
-        hnsw = build_or_load(ds.vectors, cache, 16, 200)
+    hnsw = shared_graph(ds.vectors, rank, dist, cache)
     build_s = time.perf_counter() - t_build
     gi = GpuIndex(ds.vectors, ds.cols, l0=hnsw.l0, device=local,
                   precision=_lib.FV_GPU_PREC_BF16)
@@ -331,7 +433,7 @@ def main():
 
     def routed(c):
         name, p, q, ent, bp = cls[c]
-        return routed_batch(gi, router, q, [p] * BATCH, TOPK, ent, topb=TOPK)
+        return routed_batch(gi, router, q, None, TOPK, ent, topb=TOPK, bp=bp)
 
     for i in range(args.warmup):
         routed(i % nclass)
@@ -346,23 +448,21 @@ def main():
     barrier()
     clk = Clocks(local)
     dev_ms, launches, graph_steps = 0.0, 0, 0
+    st_sum = np.zeros(3)
     results = {}
     t0 = time.perf_counter()
     for i in range(args.steps):
         c = i % nclass
         ids, dists, cnt, dec, ex, st = routed(c)
-        dev_ms += float(st.sum())
+        dev_ms += float(st[0] + st[2])  # routing runs beside the search
+        st_sum += st
         launches += int(L.pv_last_launches(gi.handle))
         graph_steps += ex
         results[c] = (ids, cnt, dec, ex)
     wall_s = time.perf_counter() - t0
     clocks = clk.stop()
     barrier()
-    if dist:
-        import torch
-        t = torch.tensor([dev_ms, wall_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, wall_s = float(t[0].item()), float(t[1].item())
+    dev_ms, wall_s = reduce_max([dev_ms, wall_s], dist, f"cuda:{local}")
     ms_per_step = dev_ms / args.steps
     value = BATCH * args.steps * world / (dev_ms / 1e3)
     e2e_qps = BATCH * args.steps * world / wall_s
@@ -443,6 +543,9 @@ def main():
             "recall_per_class": recall,
             "recall_at_10_min": round(min(v["recall_at_10"] for v in recall.values()), 4),
             "graph_batches": graph_steps,
+            "routed_stage_ms": {"bitmaps": round(st_sum[0] / args.steps, 4),
+                                "routing_beside_search": round(st_sum[1] / args.steps, 4),
+                                "search": round(st_sum[2] / args.steps, 4)},
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
                           "path": "exact FP32 scan"},
             "scan_only": {"value": round(scan_only_qps, 1), "unit": "queries/s",

@@ -597,7 +597,8 @@ GraphOut graph_out_layout(int nq, uint32_t ef) {
 int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entries,
                  const int32_t *d_qprog, const uint16_t *d_efq, uint32_t ef,
                  uint64_t max_visited, char *od, const GraphOut &lo, char *errbuf,
-                 size_t errlen) {
+                 size_t errlen, cudaStream_t st) {
+    if (!st) st = g->stream;
     const uint64_t bm_words = (g->count + 31) / 32;
     GraphScratch &gs = g->graph;
     PV_CUDA_OK(gs.visited.ensure((size_t)nq * bm_words * 4), errbuf, errlen);
@@ -629,7 +630,7 @@ int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entr
     a.out_exh = (uint8_t *)(od + lo.off_exh);
     a.stats = (uint32_t *)(od + lo.off_st);
     g->launches++;
-    PV_CUDA_OK(launch_graph(a, nq, g->stream), errbuf, errlen);
+    PV_CUDA_OK(launch_graph(a, nq, st), errbuf, errlen);
     return 0;
 }
 

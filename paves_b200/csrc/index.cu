@@ -180,11 +180,14 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
     Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
                    &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
                    &g->scan.out_d, &g->scan.out_h, &g->graph.visited, &g->graph.res,
-                   &g->graph.stats, &g->graph.route};
+                   &g->graph.stats, &g->graph.route, &g->graph.route_h, &g->graph.gout};
     for (Buf *b : bufs) b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
+    for (cudaEvent_t e : g->rev)
+        if (e) cudaEventDestroy(e);
     if (g->stream) cudaStreamDestroy(g->stream);
+    if (g->stream2) cudaStreamDestroy(g->stream2);
     delete g;
 }
 
@@ -235,6 +238,8 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         return nullptr;
     };
     if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail("stream", e);
+    if ((e = cudaStreamCreateWithFlags(&g->stream2, cudaStreamNonBlocking)) != cudaSuccess)
         return bail("stream", e);
     cudaEventCreate(&g->ev0);
     cudaEventCreate(&g->ev1);
@@ -353,7 +358,9 @@ FvGpuIndex *index_view(const FvGpuIndex *g) {
     v->sm_count = g->sm_count;
     v->view = true;
     if (cudaSetDevice(v->device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&v->stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        if (v->stream) cudaStreamDestroy(v->stream);
         delete v;
         return nullptr;
     }

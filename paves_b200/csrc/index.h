@@ -66,6 +66,8 @@ struct GraphScratch {
     Buf res;      // per query results
     Buf stats;    // per query counters
     Buf route;    // routed batches: features, logits, beam widths
+    Buf route_h{true};  // routed batches: beam widths and graph results on the host
+    Buf gout;     // routed batches: graph results on the device
 };
 
 }  // namespace pv
@@ -99,7 +101,9 @@ struct FvGpuIndex {
 
     int sm_count = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // side stream (routing beside a speculative scan)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t rev[6] = {};  // routed batches (created on first use)
     std::mutex mu;  // ABI calls are serialized per handle
 
     pv::ScanScratch scan;

@@ -127,7 +127,7 @@ GraphOut graph_out_layout(int nq, uint32_t ef);
 int graph_launch(FvGpuIndex *g, int nq, const float *d_q, const uint32_t *d_entries,
                  const int32_t *d_qprog, const uint16_t *d_efq, uint32_t ef,
                  uint64_t max_visited, char *od, const GraphOut &lo, char *errbuf,
-                 size_t errlen);
+                 size_t errlen, cudaStream_t st = nullptr);
 int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *entries,
                    const PredBatch &pb, uint32_t ef, uint64_t max_visited, FvHit *out,
                    uint32_t *out_cnt, uint8_t *exhausted, char *errbuf, size_t errlen);

@@ -840,12 +840,25 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     const uint64_t bm_words = (g->count + 31) / 32;
     ScanScratch &s = g->scan;
     const int P = db.P;
-    cudaEvent_t ev[4];
-    for (auto &e : ev) RT_OK(cudaEventCreate(&e));
-    struct EvFree {
-        cudaEvent_t *e;
-        ~EvFree() { for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]); }
-    } evf{ev};
+    cudaEvent_t *ev = g->rev;
+    for (int i = 0; i < 6; i++)
+        if (!ev[i]) RT_OK(cudaEventCreate(&ev[i]));
+    cudaStream_t side = g->stream2;
+    // size every buffer first: an allocation later would wait for the work
+    // already queued on both streams
+    const size_t hit_bytes = (size_t)nq * topb * sizeof(FvHit);
+    const size_t off_cnt = (hit_bytes + 255) & ~(size_t)255;
+    const size_t off_tr = off_cnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
+    const size_t obytes = off_tr + (size_t)nq + 256;
+    const size_t fb = ((size_t)nq * NI * 4 + 255) & ~(size_t)255;
+    const size_t zb = ((size_t)nq * NO * 4 + 255) & ~(size_t)255;
+    const size_t eb = ((size_t)nq * 2 + 255) & ~(size_t)255;
+    const size_t gbytes = have_graph ? graph_out_layout(nq, FV_GPU_MAX_EF).bytes : 0;
+    RT_OK(s.out_d.ensure(obytes));
+    RT_OK(s.out_h.ensure(obytes));
+    RT_OK(g->graph.route.ensure(fb + zb + eb));
+    RT_OK(g->graph.route_h.ensure(eb + gbytes));
+    if (have_graph) RT_OK(g->graph.gout.ensure(gbytes));
     RT_OK(cudaEventRecord(ev[0], g->stream));
     RT_OK(s.popcnt.ensure((size_t)(P > 0 ? P : 1) * 8));
     if (P > 0) {
@@ -858,52 +871,69 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                              db.ninsns, db.nconsts));
     }
     RT_OK(cudaEventRecord(ev[1], g->stream));
-    // router: features -> logits -> beam width per query (0 = scan)
-    const size_t fb = ((size_t)nq * NI * 4 + 255) & ~(size_t)255;
-    const size_t zb = ((size_t)nq * NO * 4 + 255) & ~(size_t)255;
-    RT_OK(g->graph.route.ensure(fb + zb + (size_t)nq * 2 + 256));
+    // Router on the side stream: features -> logits -> beam width per query
+    // (0 = scan), read back into pinned memory.
     float *dfeat = g->graph.route.as<float>();
     float *dz = (float *)(g->graph.route.as<char>() + fb);
     uint16_t *defq = (uint16_t *)(g->graph.route.as<char>() + fb + zb);
+    uint16_t *hefq = g->graph.route_h.as<uint16_t>();
+    RT_OK(cudaStreamWaitEvent(side, ev[1], 0));
     g->launches += plan ? 1 : 3;  // (features, MLP,) decision
     if (!plan) {
         RT_OK(launch_router_features(r, (const float *)(d + db.off_q), g->dpad, nq,
                                      s.popcnt.as<unsigned long long>(),
                                      (const int32_t *)(d + db.off_qprog), g->count,
                                      (const uint32_t *)dx, (const int32_t *)(dx + n4), dfeat,
-                                     g->stream));
-        RT_OK(launch_router_forward(r, dfeat, nq, dz, g->stream));
+                                     side));
+        RT_OK(launch_router_forward(r, dfeat, nq, dz, side));
     }
-    router_decide_kernel<<<(nq + 127) / 128, 128, 0, g->stream>>>(
+    router_decide_kernel<<<(nq + 127) / 128, 128, 0, side>>>(
         dz, nq, (const uint32_t *)dx, plan ? (const uint16_t *)(dx + 3 * n4) : nullptr, margin,
         defq);
     RT_OK(cudaGetLastError());
-    std::vector<uint16_t> efq(nq);
-    RT_OK(cudaMemcpyAsync(efq.data(), defq, (size_t)nq * 2, cudaMemcpyDeviceToHost, g->stream));
-    RT_OK(cudaStreamSynchronize(g->stream));
-    RT_OK(cudaEventRecord(ev[2], g->stream));
+    RT_OK(cudaMemcpyAsync(hefq, defq, (size_t)nq * 2, cudaMemcpyDeviceToHost, side));
+    RT_OK(cudaEventRecord(ev[2], side));
+    // Speculative scan on the main stream meanwhile: a scan costs about the
+    // same for one query as for the batch and is exact, so it runs unless
+    // a caller's plan sends every query to the graph; the router's answer
+    // only decides whether its results are replaced by the graph search's.
+    bool plan_all_graph = plan != nullptr && have_graph;
+    for (int i = 0; plan_all_graph && i < nq; i++) plan_all_graph = plan[i] > 0;
+    const bool spec = !plan_all_graph;
+    if (spec) {
+        char *od = s.out_d.as<char>();
+        const int mode = g->precision != FV_GPU_PREC_FP32 ? PV_MODE_LOW : PV_MODE_EXACT;
+        if (brute_launch(g, db, topb, mode, (FvHit *)od, (uint32_t *)(od + off_cnt),
+                         (uint8_t *)(od + off_tr), errbuf, errlen, nullptr, true))
+            return -1;
+        RT_OK(cudaEventRecord(ev[3], g->stream));
+        RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
+    }
+    RT_OK(cudaEventSynchronize(ev[2]));
     bool all_graph = have_graph;
     uint32_t efmax = 0;
     for (int i = 0; i < nq; i++) {
-        if (efq[i] == 0) all_graph = false;
-        efmax = efq[i] > efmax ? efq[i] : efmax;
+        if (hefq[i] == 0) all_graph = false;
+        efmax = hefq[i] > efmax ? hefq[i] : efmax;
     }
-    if (decided) memcpy(decided, efq.data(), (size_t)nq * 2);
+    if (decided) memcpy(decided, hefq, (size_t)nq * 2);
     if (executed) *executed = all_graph ? 1 : 0;
+    cudaEvent_t done = ev[3];
     if (all_graph) {
         const GraphOut lo = graph_out_layout(nq, efmax);
-        RT_OK(s.out_d.ensure(lo.bytes));
-        RT_OK(s.out_h.ensure(lo.bytes));
-        char *od = s.out_d.as<char>();
+        char *oh = g->graph.route_h.as<char>() + eb;
+        char *od = g->graph.gout.as<char>();
         const uint64_t mv = (uint64_t)efmax * 400 > 200000 ? (uint64_t)efmax * 400 : 200000;
         if (graph_launch(g, nq, (const float *)(d + db.off_q), (const uint32_t *)(dx + 2 * n4),
                          (const int32_t *)(d + db.off_qprog), defq, efmax, mv, od, lo, errbuf,
-                         errlen))
+                         errlen, side))
             return -1;
-        RT_OK(cudaEventRecord(ev[3], g->stream));
-        RT_OK(cudaMemcpyAsync(s.out_h.p, od, lo.bytes, cudaMemcpyDeviceToHost, g->stream));
-        RT_OK(cudaStreamSynchronize(g->stream));
-        const char *oh = s.out_h.as<char>();
+        RT_OK(cudaEventRecord(ev[4], side));
+        RT_OK(cudaMemcpyAsync(oh, od, lo.bytes, cudaMemcpyDeviceToHost, side));
+        RT_OK(cudaStreamSynchronize(side));
+        RT_OK(cudaStreamSynchronize(g->stream));  // the speculative scan, if any
+        if (spec && check_tc_watchdog(g, errbuf, errlen)) return -1;
+        g->tc_unc = nullptr;
         const uint32_t *cnt = (const uint32_t *)(oh + lo.off_cnt);
         for (int q = 0; q < nq; q++) {
             uint32_t c = cnt[q] < k[q] ? cnt[q] : k[q];
@@ -913,20 +943,12 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
         }
         g->graph_stats.resize((size_t)nq * 4);
         memcpy(g->graph_stats.data(), oh + lo.off_st, (size_t)nq * 16);
+        done = ev[4];
     } else {
-        const size_t hit_bytes = (size_t)nq * topb * sizeof(FvHit);
-        const size_t off_cnt = (hit_bytes + 255) & ~(size_t)255;
-        const size_t off_tr = off_cnt + (((size_t)nq * 4 + 255) & ~(size_t)255);
-        const size_t obytes = off_tr + (size_t)nq + 256;
-        RT_OK(s.out_d.ensure(obytes));
-        RT_OK(s.out_h.ensure(obytes));
-        char *od = s.out_d.as<char>();
-        const int mode = g->precision != FV_GPU_PREC_FP32 ? PV_MODE_LOW : PV_MODE_EXACT;
-        if (brute_launch(g, db, topb, mode, (FvHit *)od, (uint32_t *)(od + off_cnt),
-                         (uint8_t *)(od + off_tr), errbuf, errlen, nullptr, true))
+        if (!spec) {  // a plan sent every query to a graph the index lacks
+            if (errbuf && errlen) snprintf(errbuf, errlen, "routed: no graph for the plan");
             return -1;
-        RT_OK(cudaEventRecord(ev[3], g->stream));
-        RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
+        }
         RT_OK(cudaStreamSynchronize(g->stream));
         if (check_tc_watchdog(g, errbuf, errlen)) return -1;
         const char *oh = s.out_h.as<char>();
@@ -942,11 +964,19 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
         for (int q = 0; q < nq; q++)
             if (out_cnt[q] > k[q]) out_cnt[q] = k[q];
     }
-    float t[3] = {0, 0, 0};
+    // device time of the batch: bitmaps, then the search with the routing
+    // beside it (t[1] overlaps t[2]; the batch took t[0] + t[2])
+    float t[3] = {0, 0, 0}, tot = 0.f;
     cudaEventElapsedTime(&t[0], ev[0], ev[1]);
     cudaEventElapsedTime(&t[1], ev[1], ev[2]);
-    cudaEventElapsedTime(&t[2], ev[2], ev[3]);
+    cudaEventElapsedTime(&tot, ev[0], done);
+    if (all_graph && spec) {
+        float a = 0.f;  // the discarded scan may finish last
+        cudaEventElapsedTime(&a, ev[0], ev[3]);
+        if (a > tot) tot = a;
+    }
+    t[2] = tot - t[0];
     if (stage_ms) memcpy(stage_ms, t, sizeof(t));
-    g->last_kernel_ms = t[0] + t[1] + t[2];
+    g->last_kernel_ms = tot;
     return 0;
 }

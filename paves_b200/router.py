@@ -290,16 +290,19 @@ def label_actions(recall: np.ndarray, graph_ms: np.ndarray, scan_ms: float,
 
 def routed_batch(index, router: Optional[Router], queries: np.ndarray, preds, k, entries,
                  topb: Optional[int] = None, plan: Optional[np.ndarray] = None,
-                 margin: float = 0.0):
+                 margin: float = 0.0, bp: Optional[BatchPred] = None):
     """pv_routed_batch -> (ids u64 [nq][topb], dists, cnt, decided ef per query,
-    executed (1 graph / 0 scan), stage_ms [3])."""
+    executed (1 graph / 0 scan), stage_ms [3]: bitmaps, routing (beside the
+    search), search; the batch took stage_ms[0] + stage_ms[2]). bp: the
+    batch's predicate arrays with entries, if already built."""
     from .pred import concat
     L = _lib.lib()
     q = np.ascontiguousarray(queries, np.float32)
     nq = q.shape[0]
     kk = np.ascontiguousarray(np.broadcast_to(np.asarray(k, np.uint32), (nq,)))
     topb = int(kk.max()) if topb is None else int(topb)
-    bp = concat(preds, index.count, entries=entries)
+    if bp is None:
+        bp = concat(preds, index.count, entries=entries)
     pl = None if plan is None else np.ascontiguousarray(plan, np.uint16)
     out = np.zeros(nq * topb, _lib.HIT_DTYPE)
     cnt = np.zeros(nq, np.uint32)

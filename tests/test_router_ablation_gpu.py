@@ -72,8 +72,8 @@ def test_learned_router_vs_plain_rule():
                                                 plan=np.zeros(NQ, np.uint16))
         cold = plain_plan(np.full(NQ, sel), K)
         gi, _, gc, _, ex_g, st_graph = routed_batch(g, None, q, preds, K, ent, plan=cold)
-        samples += [(False, sel, float(st_scan[1:].sum()), NQ),
-                    (True, sel, float(st_graph[1:].sum()), NQ)]
+        samples += [(False, sel, float(st_scan[0] + st_scan[2]), NQ),
+                    (True, sel, float(st_graph[0] + st_graph[2]), NQ)]
         per[name] = (q, ent, preds, sel, ti, tc, cold, (gi, gc, st_graph))
     fb = feedback_from_batches(samples)
     for name, (q, ent, preds, sel, ti, tc, cold, (gi, gc, st_cold)) in per.items():
@@ -81,11 +81,11 @@ def test_learned_router_vs_plain_rule():
         warm = plain_plan(np.full(NQ, sel), K, fb)
         wi, _, wc, _, ex_w, st_w = routed_batch(g, None, q, preds, K, ent, plan=warm)
         report[name] = {
-            "learned": {"recall": _recall(li, lc, ti, tc), "ms": float(st_l.sum()),
+            "learned": {"recall": _recall(li, lc, ti, tc), "ms": float(st_l[0] + st_l[2]),
                         "graph": ex_l, "graph_frac": float((dec > 0).mean())},
-            "plain": {"recall": _recall(gi, gc, ti, tc), "ms": float(st_cold.sum()),
+            "plain": {"recall": _recall(gi, gc, ti, tc), "ms": float(st_cold[0] + st_cold[2]),
                       "ef": int(cold[0])},
-            "plain_fb": {"recall": _recall(wi, wc, ti, tc), "ms": float(st_w.sum()),
+            "plain_fb": {"recall": _recall(wi, wc, ti, tc), "ms": float(st_w[0] + st_w[2]),
                          "ef": int(warm[0])},
         }
     print(json.dumps({"scan_ms": scan_ms, "step_ms": step_ms,
@@ -96,7 +96,7 @@ def test_learned_router_vs_plain_rule():
     assert min(lr) >= min(pr) - 1e-9, report
     t_learned = sum(v["learned"]["ms"] for v in report.values())
     t_fb = sum(v["plain_fb"]["ms"] for v in report.values())
-    # the learned path pays features + MLP + reading the decision back
-    assert t_learned <= 1.25 * t_fb + 0.1 * len(report), report
+    # the learned path pays features + MLP beside its speculative scan
+    assert t_learned <= 1.25 * t_fb + 0.05 * len(report), report
     r.close()
     g.close()
