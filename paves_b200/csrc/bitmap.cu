@@ -97,6 +97,8 @@ bitmap_kernel(const double *__restrict__ cols, uint64_t nrows,
     if (threadIdx.x == 0 && s_cnt) atomicAdd(popcnt + p, (unsigned long long)s_cnt);
 }
 
+constexpr int BM_REG_COLS = 4;  // columns held in registers per row group
+
 // All programs of a batch in one pass: a warp takes 4 consecutive 32-row
 // words and evaluates every program on them, 4 rows per lane in flight, so
 // a column's values are fetched from HBM once per batch and re-read from
@@ -109,7 +111,7 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                     const PredInsn *__restrict__ insns, int ninsns,
                     const PredProg *__restrict__ progs, int P,
                     const double *__restrict__ consts, int nconsts,
-                    const int *__restrict__ dcounts,
+                    const int *__restrict__ dcounts, int ncols,
                     uint32_t *__restrict__ bitmaps, uint64_t bm_words,
                     unsigned long long *__restrict__ popcnt) {
     extern __shared__ __align__(16) unsigned char bm_smem[];
@@ -144,16 +146,38 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
             row[j] = (grp * 4 + j) * 32 + lane;
             live[j] = row[j] < nrows;
         }
+        // with few columns, each row's values are read once into registers
+        // for all programs
+        double cv[BM_REG_COLS][4];
+        if (ncols <= BM_REG_COLS) {
+#pragma unroll
+            for (int cc = 0; cc < BM_REG_COLS; cc++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    cv[cc][j] = (cc < ncols && live[j]) ? __ldg(cols + (uint64_t)cc * nrows + row[j])
+                                                         : 0.0;
+        }
         for (int p = 0; p < P; p++) {
             const PredProg pg = s_prog[p];
             uint64_t st[4] = {0, 0, 0, 0};
             for (int i = 0; i < pg.ninsn; i++) {
                 const PredInsn in = s_ins[pg.insn0 + i];
                 if (in.kind == FV_NODE_CMP || in.kind == FV_NODE_IN) {
-                    const double *c = cols + (uint64_t)in.col * nrows;
                     double v[4];
+                    if (ncols <= BM_REG_COLS) {
 #pragma unroll
-                    for (int j = 0; j < 4; j++) v[j] = live[j] ? __ldg(c + row[j]) : 0.0;
+                        for (int j = 0; j < 4; j++) {
+                            double x = cv[0][j];
+#pragma unroll
+                            for (int cc = 1; cc < BM_REG_COLS; cc++)
+                                if (in.col == cc) x = cv[cc][j];
+                            v[j] = x;
+                        }
+                    } else {
+                        const double *c = cols + (uint64_t)in.col * nrows;
+#pragma unroll
+                        for (int j = 0; j < 4; j++) v[j] = live[j] ? __ldg(c + row[j]) : 0.0;
+                    }
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
                         bool b;
@@ -208,7 +232,7 @@ constexpr size_t BM_SMEM_MAX = 200 * 1024;
 
 static cudaError_t launch_multi(const double *cols, uint64_t nrows, const PredInsn *insns,
                                 const PredProg *progs, const double *consts, int P,
-                                int ninsns, int nconsts, const int *dcounts,
+                                int ninsns, int nconsts, const int *dcounts, int ncols,
                                 uint32_t *bitmaps, uint64_t bm_words,
                                 unsigned long long *popcnt, int sm_count, cudaStream_t st) {
     const size_t smem = bitmap_multi_smem(P, ninsns, nconsts);
@@ -221,8 +245,8 @@ static cudaError_t launch_multi(const double *cols, uint64_t nrows, const PredIn
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
     bitmap_multi_kernel<<<(unsigned)blocks, 256, smem, st>>>(cols, nrows, insns, ninsns, progs, P,
-                                                             consts, nconsts, dcounts, bitmaps,
-                                                             bm_words, popcnt);
+                                                             consts, nconsts, dcounts, ncols,
+                                                             bitmaps, bm_words, popcnt);
     return cudaGetLastError();
 }
 
@@ -230,12 +254,12 @@ cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *i
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words,
                            unsigned long long *popcnt, int sm_count, cudaStream_t st,
-                           int ninsns, int nconsts) {
+                           int ninsns, int nconsts, int ncols) {
     if (P <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(popcnt, 0, sizeof(unsigned long long) * P, st);
     if (e != cudaSuccess) return e;
     if (bitmap_multi_smem(P, ninsns, nconsts) <= BM_SMEM_MAX)
-        return launch_multi(cols, nrows, insns, progs, consts, P, ninsns, nconsts, nullptr,
+        return launch_multi(cols, nrows, insns, progs, consts, P, ninsns, nconsts, nullptr, ncols,
                             bitmaps, bm_words, popcnt, sm_count, st);
     uint64_t blocks = (bm_words + 7) / 8;
     uint64_t cap = (uint64_t)sm_count * 8;
@@ -251,12 +275,13 @@ cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const Pred
                                   const PredProg *progs, const double *consts,
                                   const int *dcounts, int P_cap, int insn_cap, int const_cap,
                                   uint32_t *bitmaps, uint64_t bm_words,
-                                  unsigned long long *popcnt, int sm_count, cudaStream_t st) {
+                                  unsigned long long *popcnt, int sm_count, cudaStream_t st,
+                                  int ncols) {
     if (P_cap <= 0) return cudaSuccess;
     if (bitmap_multi_smem(P_cap, insn_cap, const_cap) > BM_SMEM_MAX) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(popcnt, 0, sizeof(unsigned long long) * P_cap, st);
     if (e != cudaSuccess) return e;
-    return launch_multi(cols, nrows, insns, progs, consts, P_cap, insn_cap, const_cap, dcounts,
+    return launch_multi(cols, nrows, insns, progs, consts, P_cap, insn_cap, const_cap, dcounts, ncols,
                         bitmaps, bm_words, popcnt, sm_count, st);
 }
 

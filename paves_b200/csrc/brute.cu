@@ -92,7 +92,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
                                          (const int *)(d + db.off_counts), P, db.ninsns,
                                          db.nconsts, s.bitmaps.as<uint32_t>(), bm_words,
                                          s.popcnt.as<unsigned long long>(), g->sm_count,
-                                         g->stream),
+                                         g->stream, g->ncols),
                    errbuf, errlen);
     } else if (P > 0) {
         PV_CUDA_OK(s.bitmaps.ensure((size_t)P * bm_words * 4), errbuf, errlen);
@@ -101,7 +101,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
                                   s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                                  db.ninsns, db.nconsts),
+                                  db.ninsns, db.nconsts, g->ncols),
                    errbuf, errlen);
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);

@@ -18,7 +18,8 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
 cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words, unsigned long long *popcnt,
-                           int sm_count, cudaStream_t st, int ninsns, int nconsts);
+                           int sm_count, cudaStream_t st, int ninsns, int nconsts,
+                           int ncols = 1 << 30);
 // Same, with the batch's {P, ninsns, nconsts} read on the device from
 // dcounts (each at most its cap): one launch shape for a CUDA graph.
 size_t bitmap_multi_smem(int P, int ninsns, int nconsts);
@@ -26,7 +27,8 @@ cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const Pred
                                   const PredProg *progs, const double *consts,
                                   const int *dcounts, int P_cap, int insn_cap, int const_cap,
                                   uint32_t *bitmaps, uint64_t bm_words,
-                                  unsigned long long *popcnt, int sm_count, cudaStream_t st);
+                                  unsigned long long *popcnt, int sm_count, cudaStream_t st,
+                                  int ncols = 1 << 30);
 
 // ---- exact FP32 scan (scan_f32.cu)
 struct ScanF32Args {
@@ -64,7 +66,7 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
                          uint8_t *trunc, cudaStream_t st,
                          unsigned long long *tau_out = nullptr, int kout = 0,
-                         uint8_t *unc = nullptr);
+                         uint8_t *unc = nullptr, int kuse = 0);
 
 // ---- batch staging (brute.cu)
 struct DevBatch {

@@ -42,15 +42,38 @@ static_assert(P_N == PV_MLP_NPARAMS, "parameter layout");
 
 // ---------------------------------------------------------------- features
 // One CTA per query; warp w scores centroids w, w+8, ... with lanes across
-// dimensions, keeps a sorted top-8 per lane, and warp 0 merges the lists.
+// dimensions and keeps a sorted top-8 per lane; each warp reduces its
+// lanes' lists to a top-8 by 8 rounds of warp-wide minimum, and warp 0 does
+// the same over the 8 warps' lists. Under 1 KB of shared memory, so the
+// kernel can run beside a scan that holds most of each SM's.
+__device__ __forceinline__ float pick8(const float (&t)[8], int i) {
+    float v = INFINITY;
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        if (j == i) v = t[j];
+    return v;
+}
+
+__device__ __forceinline__ void warp_argmin(float &best, int &who) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int ow = __shfl_xor_sync(0xffffffffu, who, o);
+        if (ov < best || (ov == best && ow < who)) {
+            best = ov;
+            who = ow;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) router_features_kernel(
     const float *__restrict__ queries, int dpad, const float *__restrict__ cent, int ncent,
     const unsigned long long *__restrict__ popcnt, const int32_t *__restrict__ qprog,
     uint64_t nrows, const uint32_t *__restrict__ kq, const int32_t *__restrict__ kind,
     float *__restrict__ feats) {
     extern __shared__ float rsm[];
-    float *sq = rsm;                    // [dpad]
-    float *cand = sq + dpad;            // [8 warps][32 lanes][8] distances
+    float *sq = rsm;              // [dpad]
+    __shared__ float cand[64];    // [8 warps][8]
     __shared__ float s_norm;
     const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int j = tid; j < dpad; j += blockDim.x) sq[j] = queries[(uint64_t)q * dpad + j];
@@ -87,45 +110,30 @@ __global__ void __launch_bounds__(256) router_features_kernel(
             }
         }
     }
-#pragma unroll
-    for (int i = 0; i < 8; i++) cand[(warp * 32 + lane) * 8 + i] = top[i];
+    // the warp's 8 smallest: 8 rounds of minimum over the lanes' list heads
+    {
+        int head = 0;
+        float mine = INFINITY;
+        for (int r = 0; r < 8; r++) {
+            float best = head < 8 ? pick8(top, head) : INFINITY;
+            int who = lane;
+            warp_argmin(best, who);
+            if (lane == who) head++;
+            if (lane == r) mine = best;
+        }
+        if (lane < 8) cand[warp * 8 + lane] = mine;
+    }
     __syncthreads();
     if (warp == 0) {
-        // 256 sorted lists of 8; each lane merges 8 lists into a sorted 8
-        float m[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) m[i] = INFINITY;
-        for (int l = lane; l < 256; l += 32)
-            for (int i = 0; i < 8; i++) {
-                float v = cand[l * 8 + i];
-                if (!(v < m[7])) break;
-#pragma unroll
-                for (int t = 0; t < 8; t++) {
-                    const float u = m[t];
-                    const bool sw = v < u;
-                    m[t] = sw ? v : u;
-                    v = sw ? u : v;
-                }
-            }
-        // 8 rounds of warp-wide minimum over the lanes' list heads
-        int head = 0;
+        float v0 = cand[lane], v1 = cand[lane + 32];
         float out = 0.f;
         for (int r = 0; r < 8; r++) {
-            float v = INFINITY;
-#pragma unroll
-            for (int i = 0; i < 8; i++)
-                if (i == head) v = m[i];
-            float best = v;
+            float best = fminf(v0, v1);
             int who = lane;
-            for (int o = 16; o; o >>= 1) {
-                const float ov = __shfl_xor_sync(0xffffffffu, best, o);
-                const int ow = __shfl_xor_sync(0xffffffffu, who, o);
-                if (ov < best || (ov == best && ow < who)) {
-                    best = ov;
-                    who = ow;
-                }
+            warp_argmin(best, who);
+            if (lane == who) {  // remove one occurrence of the minimum
+                if (v0 <= v1) v0 = INFINITY; else v1 = INFINITY;
             }
-            if (lane == who) head++;
             if (lane == r) out = best;
         }
         float *f = feats + (uint64_t)q * NI;
@@ -205,6 +213,47 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(
     }
 #pragma unroll
     for (int o = 0; o < NO; o++) Z3[(uint64_t)s * NO + o] = z3[o];
+}
+
+// Inference: one warp per sample, lanes over the hidden units, weights
+// read through L1 (no shared memory, so it runs beside a scan). Its sums
+// are ordered differently from mlp_forward_kernel's (training) ones.
+__global__ void __launch_bounds__(256) mlp_infer_kernel(const float *__restrict__ X, int n,
+                                                       const __nv_bfloat16 *__restrict__ w,
+                                                       const float *__restrict__ norm,
+                                                       float *__restrict__ Z3) {
+    const int s = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= n) return;
+    const float xi =
+        lane < NI ? (X[(uint64_t)s * NI + lane] - __ldg(norm + lane)) / __ldg(norm + NI + lane)
+                  : 0.f;
+    float h0 = __bfloat162float(w[P_B1 + lane]), h1 = __bfloat162float(w[P_B1 + lane + 32]);
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const float xb = __shfl_sync(0xffffffffu, xi, i);
+        h0 = fmaf(xb, __bfloat162float(w[P_W1 + i * NH + lane]), h0);
+        h1 = fmaf(xb, __bfloat162float(w[P_W1 + i * NH + lane + 32]), h1);
+    }
+    h0 = fmaxf(h0, 0.f);
+    h1 = fmaxf(h1, 0.f);
+    float g0 = __bfloat162float(w[P_B2 + lane]), g1 = __bfloat162float(w[P_B2 + lane + 32]);
+#pragma unroll 8
+    for (int i = 0; i < NH; i++) {
+        const float hb = __shfl_sync(0xffffffffu, i < 32 ? h0 : h1, i & 31);
+        g0 = fmaf(hb, __bfloat162float(w[P_W2 + i * NH + lane]), g0);
+        g1 = fmaf(hb, __bfloat162float(w[P_W2 + i * NH + lane + 32]), g1);
+    }
+    g0 = fmaxf(g0, 0.f);
+    g1 = fmaxf(g1, 0.f);
+#pragma unroll
+    for (int o = 0; o < NO; o++) {
+        float p = g0 * __bfloat162float(w[P_W3 + lane * NO + o]);
+        p = fmaf(g1, __bfloat162float(w[P_W3 + (lane + 32) * NO + o]), p);
+#pragma unroll
+        for (int x = 16; x; x >>= 1) p += __shfl_xor_sync(0xffffffffu, p, x);
+        if (lane == 0) Z3[(uint64_t)s * NO + o] = p + __bfloat162float(w[P_B3 + o]);
+    }
 }
 
 // Softmax cross-entropy: dZ3 = w_s (p - onehot) / W, W = sum of the batch's
@@ -466,7 +515,7 @@ int router_kind(const FvGpuPredNode *nodes, int nnodes, int32_t root) {
     }
 }
 
-size_t router_features_smem(int dpad) { return (size_t)(dpad + 256 * 8) * 4; }
+size_t router_features_smem(int dpad) { return (size_t)dpad * 4; }
 
 cudaError_t launch_router_features(const PvRouter *r, const float *d_q, int dpad, int nq,
                                    const unsigned long long *popcnt, const int32_t *qprog,
@@ -484,9 +533,7 @@ cudaError_t launch_router_features(const PvRouter *r, const float *d_q, int dpad
 
 cudaError_t launch_router_forward(const PvRouter *r, const float *feats, int n, float *Z3,
                                   cudaStream_t st) {
-    mlp_forward_kernel<<<(n + 127) / 128, 128, 0, st>>>(feats, nullptr, nullptr, n, r->mlp.w,
-                                                        r->mlp.norm, nullptr, nullptr, nullptr,
-                                                        Z3);
+    mlp_infer_kernel<<<(n + 7) / 8, 256, 0, st>>>(feats, n, r->mlp.w, r->mlp.norm, Z3);
     return cudaGetLastError();
 }
 
@@ -536,7 +583,7 @@ extern "C" int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const floa
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
                              bm_words, s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                             db.ninsns, db.nconsts));
+                             db.ninsns, db.nconsts, g->ncols));
     }
     const size_t fbytes = (size_t)nq * NI * 4;
     RT_OK(s.out_d.ensure(fbytes));
@@ -868,7 +915,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
                              bm_words, s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                             db.ninsns, db.nconsts));
+                             db.ninsns, db.nconsts, g->ncols));
     }
     RT_OK(cudaEventRecord(ev[1], g->stream));
     // Router on the side stream: features -> logits -> beam width per query

@@ -208,7 +208,7 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
              const unsigned long long *__restrict__ popcnt, uint64_t nrows,
              FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
              uint8_t *__restrict__ trunc, unsigned long long *__restrict__ tau_out,
-             int KO, uint8_t *__restrict__ unc) {
+             int KO, uint8_t *__restrict__ unc, int KU) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *buf = (uint64_t *)smem_raw;   // [M]
     int *s_c = (int *)(buf + M);            // [grow] prefix lengths
@@ -226,7 +226,7 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
     // then sorted. Taken whenever they fit the buffer (the usual case).
     for (int g = tid; g < grow; g += blockDim.x) {
         const uint32_t c = cnts[g];
-        s_c[g] = c > (uint32_t)K ? K : (int)c;
+        s_c[g] = c > (uint32_t)KU ? KU : (int)c;
     }
     if (tid == 0) s_n = 0;
     __syncthreads();
@@ -269,7 +269,7 @@ merge_kernel(const uint64_t *__restrict__ part, const uint32_t *__restrict__ par
     // general path: measure each list's prefix, then fold in rounds
     for (int g = warp; g < grow; g += nwarps) {
         int c = (int)cnts[g];
-        if (c > K) c = K;
+        if (c > KU) c = KU;
         const uint64_t *L = lists + (uint64_t)g * K;
         int n = 0;
         for (int j0 = 0; j0 < c; j0 += 32) {
@@ -482,15 +482,16 @@ cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int gro
                          const int32_t *qprog, const unsigned long long *popcnt,
                          uint64_t nrows, int nq, FvHit *out, uint32_t *out_cnt,
                          uint8_t *trunc, cudaStream_t st, unsigned long long *tau_out,
-                         int kout, uint8_t *unc) {
+                         int kout, uint8_t *unc, int kuse) {
     if (kout <= 0) kout = K;
+    if (kuse <= 0 || kuse > K) kuse = K;
     if (kout > pl.M) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)pl.merge_smem);
     if (e != cudaSuccess) return e;
     merge_kernel<<<nq, 256, pl.merge_smem, st>>>(part, part_cnt, grow, K, pl.M, tau, qprog,
                                                  popcnt, nrows, out, out_cnt, trunc, tau_out,
-                                                 kout, unc);
+                                                 kout, unc, kuse);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,8 @@
 // Warp roles (192 threads): warp 0 TMA producer, warp 1 TMEM allocator +
 // MMA issuer, warps 2-5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).
 // All waits are bounded by a deadline and unwind through an abort flag.
+#include <algorithm>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -48,6 +50,7 @@ constexpr int TC_KBS = 2;           // K-blocks per pipeline stage
 // certifies per query (queries it cannot certify are re-run exactly).
 constexpr int TC_MAX_SUPERSET = 1024;
 constexpr int TC_MAX_LIST = 64;
+constexpr int TC_MAX_STAGES = 8;   // TMA pipeline stages at most
 
 template <bool FP8>
 __device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
@@ -101,7 +104,9 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     unsigned char *sQ = base;                                  // KBt boxes
     unsigned char *sX = sQ + (size_t)KBt * TC_BOX;             // NS * KBS boxes
     // per (query, row half) lists [KP][128*EPI] and candidate staging [32][128*EPI]
-    uint64_t *lists = (uint64_t *)(sX + (size_t)NS * TC_KBS * TC_BOX);
+    // a stage holds one K-chunk of a row tile: min(TC_KBS, KBt) boxes
+    const size_t SB = (size_t)(KBt < TC_KBS ? KBt : TC_KBS) * TC_BOX;
+    uint64_t *lists = (uint64_t *)(sX + (size_t)NS * SB);
     float *stage = (float *)(lists + (size_t)TC_BM * EPI * KP);
     uint64_t *bars = (uint64_t *)(stage + 32 * TC_BM * EPI);
     uint64_t *full = bars;            // [NS]
@@ -168,7 +173,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     const int nkb = min(TC_KBS, KBt - kc * TC_KBS);
                     mbar_arrive_expect_tx(&full[s], (uint32_t)nkb * TC_BOX);
                     for (int kb = 0; kb < nkb; kb++)
-                        tma_load_2d(sX + ((size_t)s * TC_KBS + kb) * TC_BOX, &tmX,
+                        tma_load_2d(sX + (size_t)s * SB + (size_t)kb * TC_BOX, &tmX,
                                     (kc * TC_KBS + kb) * (FP8 ? 128 : 64), y, &full[s]);
                 }
                 if (a.trace && blockIdx.x == 0 && t < (uint64_t)a.trace_tiles)
@@ -207,7 +212,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     const int nkb = min(TC_KBS, KBt - kc * TC_KBS);
                     for (int kb = 0; kb < nkb; kb++) {
                         const uint64_t ad = desc_sw128(sQ + (size_t)(kc * TC_KBS + kb) * TC_BOX);
-                        const uint64_t bd = desc_sw128(sX + ((size_t)s * TC_KBS + kb) * TC_BOX);
+                        const uint64_t bd = desc_sw128(sX + (size_t)s * SB + (size_t)kb * TC_BOX);
 #pragma unroll
                         for (int kk = 0; kk < 4; kk++)  // 4 x 32 bytes of K per block
                             mma_f16_or_f8<FP8>(dcol, ad + 2 * kk, bd + 2 * kk, idesc,
@@ -248,7 +253,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         // the same slot index hit 32 different banks
         uint64_t *L = lists + slot;
 #define PV_L(j) L[(size_t)(j) * NSLOT]
-        int n = 0, wi = 0;
+        int n = 0;
         uint64_t lmax = KEY_MAX;   // worst kept key once the list is full
         uint64_t thr = qvalid ? KEY_MAX : 0ull;  // admission threshold
         float thr_d = qvalid ? __int_as_float(0x7f800000) : -1.f;  // its distance
@@ -325,22 +330,39 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     // <= : the seeded bound is itself a row key that this
                     // pass must admit again (keys are unique)
                     if (key > thr) continue;
+                    // the list is a max-heap (root = worst kept key): an
+                    // admission costs O(log KP) shared-memory steps
                     if (n < KP) {
-                        PV_L(n) = key;
-                        n++;
+                        int j = n++;
+                        while (j > 0) {
+                            const int p = (j - 1) >> 1;
+                            const uint64_t pv = PV_L(p);
+                            if (pv >= key) break;
+                            PV_L(j) = pv;
+                            j = p;
+                        }
+                        PV_L(j) = key;
                         if (n < KP) continue;
                     } else {
-                        PV_L(wi) = key;
-                    }
-                    wi = 0;
-                    lmax = PV_L(0);
-                    for (int j = 1; j < KP; j++) {
-                        const uint64_t v = PV_L(j);
-                        if (v > lmax) {
-                            lmax = v;
-                            wi = j;
+                        int j = 0;
+                        for (;;) {
+                            int ch = 2 * j + 1;
+                            if (ch >= KP) break;
+                            uint64_t cv = PV_L(ch);
+                            if (ch + 1 < KP) {
+                                const uint64_t c2 = PV_L(ch + 1);
+                                if (c2 > cv) {
+                                    cv = c2;
+                                    ch++;
+                                }
+                            }
+                            if (cv <= key) break;
+                            PV_L(j) = cv;
+                            j = ch;
                         }
+                        PV_L(j) = key;
                     }
+                    lmax = PV_L(0);
                     if (lmax < thr) {
                         thr = lmax;
                         thr_d = key_dist(lmax);
@@ -364,15 +386,27 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             atomicExch(a.err, 3);
         }
         if (qvalid) {
-            // ascending list (insertion sort, <= KP entries)
-            for (int i = 1; i < n; i++) {
-                const uint64_t v = PV_L(i);
-                int j = i - 1;
-                while (j >= 0 && PV_L(j) > v) {
-                    PV_L(j + 1) = PV_L(j);
-                    j--;
+            // heap -> ascending list (heapsort in place)
+            for (int end = n - 1; end > 0; end--) {
+                const uint64_t top = PV_L(0), v = PV_L(end);
+                PV_L(end) = top;
+                int j = 0;
+                for (;;) {
+                    int ch = 2 * j + 1;
+                    if (ch >= end) break;
+                    uint64_t cv = PV_L(ch);
+                    if (ch + 1 < end) {
+                        const uint64_t c2 = PV_L(ch + 1);
+                        if (c2 > cv) {
+                            cv = c2;
+                            ch++;
+                        }
+                    }
+                    if (cv <= v) break;
+                    PV_L(j) = cv;
+                    j = ch;
                 }
-                PV_L(j + 1) = v;
+                PV_L(j) = v;
             }
             // partial list (rgrp, half) of query qg; the merge sees grow*EPI lists
             const uint64_t li = (uint64_t)qg * a.grow * EPI + (uint64_t)rgrp * EPI + half;
@@ -551,13 +585,14 @@ bool tc_supported(const FvGpuIndex *g) {
 }
 
 static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
-    return 1024 + (size_t)kblocks * TC_BOX + (size_t)NS * TC_KBS * TC_BOX +
+    return 1024 + (size_t)kblocks * TC_BOX +
+           (size_t)NS * (kblocks < TC_KBS ? kblocks : TC_KBS) * TC_BOX +
            (size_t)TC_BM * EPI * KP * 8 + (size_t)32 * TC_BM * EPI * 4 +
            (size_t)(2 * NS + 6) * 8;
 }
 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
-    if (!tc_supported(g) || (epi != 1 && epi != 2) || ns < 2 || ns > 4) return false;
+    if (!tc_supported(g) || (epi != 1 && epi != 2) || ns < 2 || ns > TC_MAX_STAGES) return false;
     const int S = tc_superset(g, topb, -1.f);
     if (!S) return false;
     const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
@@ -602,16 +637,20 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     // two epilogue warp groups (each row half of a tile) when the lists fit,
     // with at least two pipeline stages; else one group
     const size_t smem_cap = 227 * 1024;
-    int EPI = 2, NS = 4;
+    // stages: up to 128 KB of rows in flight
+    const int ns0 = std::min(TC_MAX_STAGES, std::max(
+        2, (int)(128 * 1024 / ((size_t)std::min(kblocks, TC_KBS) * TC_BOX))));
+    int EPI = 2, NS = ns0;
     while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
     if (tc_smem(kblocks, NS, KP, EPI) > smem_cap) {
         EPI = 1;
-        NS = 4;
+        NS = ns0;
         while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
     }
     if (g->tune_epi || g->tune_ns) {  // a tuned shape, if it fits
         const int e = g->tune_epi ? g->tune_epi : EPI, n = g->tune_ns ? g->tune_ns : NS;
-        if ((e == 1 || e == 2) && n >= 2 && n <= 4 && tc_smem(kblocks, n, KP, e) <= smem_cap) {
+        if ((e == 1 || e == 2) && n >= 2 && n <= TC_MAX_STAGES &&
+            tc_smem(kblocks, n, KP, e) <= smem_cap) {
             EPI = e;
             NS = n;
         }
@@ -699,22 +738,32 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
-    // Seeding pass: one tile per CTA from an evenly strided sample; the
+    // Seeding pass: a few tiles per CTA from an evenly strided sample; the
     // merged K'-th key of the sample bounds the K'-th key of the whole
     // scan, so the main pass admits only rows that can still matter.
     if (ntiles_all >= 8 * (uint64_t)grow) {
         TcArgs sa = a;
-        sa.tile0_mul = ntiles_all / grow;
-        sa.tile_step = 1;
-        sa.tiles_per_cta = 1;
+        // larger supersets take a larger sample (up to 8 tiles per CTA,
+        // spread over the CTA's own range), so the bound stays near the
+        // S-th key and the final merge's survivors fit one pass
+        const uint64_t region = ntiles_all / grow;
+        const uint64_t m = std::min<uint64_t>(std::min<uint64_t>(8, region),
+                                              std::max<uint64_t>(1, ((uint64_t)S + 15) / 16));
+        sa.tile0_mul = region;
+        sa.tile_step = std::max<uint64_t>(1, region / m);
+        sa.tiles_per_cta = m;
         g->launches += 2;  // seeding pass + its merge
         PV_CUDA_OK(run(sa), errbuf, errlen);
         ScanPlan sp;
         sp.M = 4096;
         sp.merge_smem = (size_t)sp.M * 8 + (size_t)nlists * 8;
+        // only each list's best keys: the S-th key of a subset of the
+        // sample still bounds the S-th key of the scan, and the subset
+        // fits the merge buffer in one pass
+        const int kuse = std::max(1, std::min(KP, sp.M / std::max(1, nlists)));
         PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, sp, a.tau, d_qprog, popcnt,
                                 g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
-                                a.tau, S),
+                                a.tau, S, nullptr, kuse),
                    errbuf, errlen);
     }
     // stage boundary: everything before the main pass (bitmaps, query prep,

@@ -241,7 +241,7 @@ int autotune(PvStream *s, const float *tq, int ntq, char *errbuf, size_t errlen)
             const int qtiles = (b->B + 127) / 128;
             const int g1 = std::max(1, v->sm_count / qtiles);
             for (int epi : {1, 2})
-                for (int ns : {2, 3, 4})
+                for (int ns : {2, 3, 4, 6, 8})
                     if (tc_shape_fits(v, b->topb, epi, ns))
                         for (int grow : {g1, std::max(1, g1 / 2)})
                             cands.push_back({PV_MODE_LOW, epi, ns, grow});
