@@ -228,21 +228,43 @@ KERNEL_CASES = {
     "exact_b1": (1, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, 5),
     "exact_b64": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, None),
     "bf16_b64": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, None),
+    "fp8_b64": (64, _lib.FV_GPU_PREC_FP8, _lib.PV_MODE_LOW, None),
+    # graph: 200k x 128 rows, HNSW M=16 efC=100, 64 queries, 10% filter, ef 64
+    "graph_b64": (64, None, None, None),
 }
 
 
-def kernel_case(name, iters):
-    """One batch shape run `iters` times (device-resident inputs): the
-    small, self-contained program that ncu captures profile."""
+def kernel_case(name, iters, tc_shape=None):
+    """One batch shape run `iters` times after 3 warm-up runs (device-
+    resident inputs): the small, self-contained program that ncu captures
+    profile. tc_shape = (epi, stages, grow, replicas), 0 = automatic."""
     nq, prec, mode, pk = KERNEL_CASES[name]
+    if name == "graph_b64":
+        from paves_b200.hnsw import Hnsw
+        ds = datagen.make_dataset(200_000, DIM, nq=nq)
+        h = Hnsw(ds.vectors, 16, 100)
+        gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
+        p = datagen.graph_predicates()["sel10%"]
+        ent = h.entries(ds.queries)
+        ms = 0.0
+        for _ in range(iters):
+            gi.graph_batch(ds.queries, ent, [p] * nq, 64)
+            ms += _lib.lib().pv_last_kernel_ms(gi.handle)
+        print(json.dumps({"case": name, "iters": iters, "ms": round(ms / iters, 4)}))
+        gi.close()
+        return
     ds, classes, _ = make_workload(nb=max(nq, 1))
     if pk is not None:
         preds = [classes[pk][1]] * nq
     else:
         preds = [classes[q % len(classes)][1] for q in range(nq)]
     gi = GpuIndex(ds.vectors, ds.cols, precision=prec)
+    if tc_shape:
+        if _lib.lib().pv_tc_shape(gi.handle, *tc_shape) != 0:
+            raise ValueError(f"bad tensor-core shape {tc_shape}")
     bp = pred.concat(preds[:nq], N_ROWS)
     b = prepared_batch(gi, ds.queries[:nq], bp, TOPK, mode)
+    batch_run(b, 3)
     _, st = batch_run(b, iters, stages=True)
     print(json.dumps({"case": name, "iters": iters,
                       "stage_ms": [round(x / iters, 4) for x in st]}))
@@ -332,6 +354,76 @@ def stream_bench(args):
     gi.close()
 
 
+def graph_bench(args):
+    """Filtered graph search: the 1M x 128 set, HNSW (M=16, efConstruction
+    200) built by the library, 64 queries per batch, filters at 1%, 10% and
+    50%, ef in {32, 64, 128, 256}; recall@10 against the exact scan and
+    device-time QPS, beside the reference engine's HnswCursor (built from
+    its sources) on the same graph file, one query per host thread."""
+    from concurrent.futures import ThreadPoolExecutor
+    ds, _, _ = make_workload()
+    cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
+    h = shared_graph(ds.vectors, 0, None, cache)
+    gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
+    L = _lib.lib()
+    q = ds.queries[:BATCH]
+    ent = h.entries(q)
+    res = []
+    for name, p in datagen.graph_predicates().items():
+        preds = [p] * BATCH
+        xi, _, xc, _ = gi.brute_batch(q, preds, TOPK)
+        for ef in (32, 64, 128, 256):
+            for _ in range(max(1, args.warmup)):
+                gi.graph_batch(q, ent, preds, ef)
+            dev = 0.0
+            reps = max(1, min(args.steps, 10))
+            for _ in range(reps):
+                ids, _, cnt, _ = gi.graph_batch(q, ent, preds, ef)
+                dev += L.pv_last_kernel_ms(gi.handle)
+            rec = float(np.mean([np.isin(xi[i, :xc[i]], ids[i, :TOPK]).sum() / max(1, int(xc[i]))
+                                 for i in range(BATCH)]))
+            st = np.zeros(BATCH * 4, np.uint32)
+            L.pv_graph_stats(gi.handle, _lib.ptr(st), BATCH)
+            st = st.reshape(BATCH, 4)
+            res.append({"filter": name, "ef": ef, "recall_at_10": round(rec, 4),
+                        "qps": round(BATCH * reps / (dev / 1e3), 1),
+                        "mean_steps": round(float(st[:, 0].mean()), 1),
+                        "mean_visited": round(float(st[:, 1].mean()), 1)})
+    ref = []
+    try:
+        from oracle import refengine
+        if refengine.available("cpu"):
+            path = os.path.join(tempfile.gettempdir(), "paves_bench_graph.idx")
+            h.write(path, ds.cols)
+            R = refengine.RefIndex(path)
+            thr = os.cpu_count() or 1
+            for name, p in datagen.graph_predicates().items():
+                ph = R.compile(p)
+                xi, _, xc, _ = gi.brute_batch(q, [p] * BATCH, TOPK)
+                for ef in (32, 64, 128, 256):
+                    t0 = time.perf_counter()
+                    with ThreadPoolExecutor(thr) as ex:
+                        outs = list(ex.map(lambda i: R.hnsw(q[i], ph, TOPK, ef)[0], range(BATCH)))
+                    wall = time.perf_counter() - t0
+                    rec = float(np.mean([np.isin(xi[i, :xc[i]], outs[i]).sum() / max(1, int(xc[i]))
+                                         for i in range(BATCH)]))
+                    ref.append({"filter": name, "ef": ef, "recall_at_10": round(rec, 4),
+                                "qps": round(BATCH / wall, 1), "threads": thr})
+                R.free_pred(ph)
+            R.close()
+    except Exception as e:  # the reference arm is informative only
+        ref = [{"failed": str(e)}]
+    line = {"metric": "filtered graph search QPS, 1M x 128 L2, HNSW level 0", "unit": "queries/s",
+            "value": max(r["qps"] for r in res), "higher_is_better": True, "n_gpus": 1,
+            "data": "synthetic",
+            "config": {"workload": "1M x 128 Gaussian-mixture rows, HNSW M=16 efC=200 built by "
+                                   "the library, 64-query batches, filters 1%/10%/50%, top-10",
+                       "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK},
+            "results": res, "reference_cpu": ref}
+    print(json.dumps(line), flush=True)
+    gi.close()
+
+
 def shared_graph(vectors, rank, dist, cache):
     """Rank 0 builds the HNSW graph (or reloads this host's cached copy);
     after a barrier the other ranks load rank 0's copy instead of building
@@ -362,16 +454,23 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="headline", choices=["headline", "stream"],
-                    help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency)")
+    ap.add_argument("--workload", default="headline", choices=["headline", "stream", "graph"],
+                    help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency); "
+                         "graph: filtered HNSW search at ef 32..256 beside the reference cursor")
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES),
                     help="run one batch shape --steps times and exit (for profilers)")
+    ap.add_argument("--tc-shape", default=None,
+                    help="kernel cases: tensor-core shape epi,stages,grow,replicas (0 = auto)")
     args = ap.parse_args()
     if args.workload == "stream":
         stream_bench(args)
         return
+    if args.workload == "graph":
+        graph_bench(args)
+        return
     if args.kernel_case:
-        kernel_case(args.kernel_case, max(1, args.steps))
+        shape = tuple(int(x) for x in args.tc_shape.split(",")) if args.tc_shape else None
+        kernel_case(args.kernel_case, max(1, args.steps), shape)
         return
     args.warmup = max(3, args.warmup)
 
@@ -478,17 +577,25 @@ def main():
                         "path": "graph" if ex else "bf16-scan",
                         "graph_queries": int((dec > 0).sum())}
 
-    # the tensor-core scan kernel alone (each class batch, prepared)
-    scan_ms, st_tot, superset = 0.0, [0.0] * 4, 0
+    # the scan path without the router (each class batch, prepared); the
+    # roofline averages the tensor-core kernel over the classes that run it
+    # (selective classes take the sparse route: an exact scan of their rows)
+    st_tot, st_tc, n_tc, superset, per_cls = [0.0] * 4, [0.0] * 4, 0, 0, {}
     for name, p, q, ent, bp in cls:
         b = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_LOW)
         batch_run(b, 3)
         _, st = batch_run(b, per_class, stages=True)
+        sparse = bool(L.pv_last_sparse(gi.handle))
         st_tot = [x + y for x, y in zip(st_tot, st)]
-        superset = int(L.pv_last_superset(gi.handle))
+        if not sparse:
+            st_tc = [x + y for x, y in zip(st_tc, st)]
+            n_tc += per_class
+            superset = int(L.pv_last_superset(gi.handle))
+        per_cls[name] = {"route": "sparse" if sparse else "tensor-core",
+                         "ms": round(sum(st) / per_class, 4)}
         L.pv_batch_free(b)
     nrun = per_class * nclass
-    scan_ms = st_tot[1] / nrun
+    scan_ms = st_tc[1] / max(1, n_tc)
     scan_only_qps = BATCH * nrun / (sum(st_tot) / 1e3)
     hbm, bf16, peak_kind = load_peaks()
     # tensor-core scan: bf16 rows (128 dims = 256 B) + f32 norm, once per batch
@@ -549,16 +656,17 @@ def main():
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
                           "path": "exact FP32 scan"},
             "scan_only": {"value": round(scan_only_qps, 1), "unit": "queries/s",
-                          "path": "bf16 scan + re-rank, no router"},
+                          "path": "bf16 scan + re-rank (sparse route for selective "
+                                  "filters), no router", "classes": per_cls},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(achieved / hbm, 4),
                          "traffic": load_traffic("scan_tc_kernel"),
                          "kernel": "scan_tc_kernel", "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
             "scan_gbs_batch1": round(scan_gbs_b1, 1),
-            "stage_ms": {"bitmap+prep+seed": round(st_tot[0] / nrun, 4),
+            "stage_ms": {"bitmap+prep+seed": round(st_tc[0] / max(1, n_tc), 4),
                          "scan": round(scan_ms, 4),
-                         "merge+rerank": round(st_tot[2] / nrun, 4)},
+                         "merge+rerank": round(st_tc[2] / max(1, n_tc), 4)},
             "hnsw_build_s": round(build_s, 1),
             "clocks": clocks,
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,

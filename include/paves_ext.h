@@ -305,6 +305,24 @@ int pv_last_superset(const FvGpuIndex *g);
  * only reports them. */
 int pv_last_uncertain(const FvGpuIndex *g);
 
+/* Selective filters: a batch whose queries share one filter that the
+ * index's sorted attribute values bound to at most max(4096, count / 16)
+ * matching rows scans only those rows (the bitmap compacted to a row list,
+ * then the exact FP32 scan over the list) — the reference's posting-list
+ * driver route (engine.cpp:464-599, gpu_engine.cu:2249-2260). Results are
+ * those of the full scan. pv_last_sparse: 1 if the last brute batch on g
+ * took this route. pv_filter_bound: the bound for one filter (node 0 is
+ * the root; nnodes 0 = no filter -> count). */
+int pv_last_sparse(const FvGpuIndex *g);
+/* Shape of the tensor-core scan for later batches on g (0 = automatic):
+ * epilogue warp groups (1, 2), pipeline stages (2..8), CTAs along rows per
+ * query tile, query replicas down the tile (1, 2, 4; capped so that each
+ * replica's share of a 128-row tile is at least 32 rows). -1: bad value. */
+int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep);
+int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
+                    const int32_t *children, int nchildren, const double *invals, int ninvals,
+                    uint64_t *bound, char *errbuf, size_t errlen);
+
 /* Kernels launched by the last batch call on g (summed over the iterations
  * of pv_batch_run). */
 int pv_last_launches(const FvGpuIndex *g);

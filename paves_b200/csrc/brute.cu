@@ -57,6 +57,18 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
     if (!pb.insns.empty())
         memcpy(h + db.off_insns, pb.insns.data(), pb.insns.size() * sizeof(PredInsn));
     if (!pb.consts.empty()) memcpy(h + db.off_consts, pb.consts.data(), pb.consts.size() * 8);
+    // sparse route: one filter shared by the whole batch whose matches are
+    // bounded by a small count (the scan then reads only those rows)
+    db.sparse_bound = 0;
+    if (P == 1 && !g->sorted_cols.empty()) {
+        bool all = true;
+        for (int q = 0; q < nq && all; q++) all = pb.qprog[q] == 0;
+        if (all) {
+            const uint64_t b = prog_upper_bound(g, pb.insns.data() + pb.progs[0].insn0,
+                                                pb.progs[0].ninsn, pb.consts.data());
+            if (b <= sparse_limit(g->count)) db.sparse_bound = b;
+        }
+    }
     return 0;
 }
 
@@ -105,6 +117,21 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
                    errbuf, errlen);
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
+    }
+    g->last_sparse = 0;
+    if (db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024) {
+        g->tc_err = nullptr;
+        g->tc_unc = nullptr;
+        g->last_sparse = 1;
+        if (ev) cudaEventRecord(ev[1], g->stream);
+        if (sparse_launch(g, db, topb, db.sparse_bound, d_out, d_cnt, d_trunc, errbuf, errlen))
+            return -1;
+        if (ev) {
+            cudaEventRecord(ev[2], g->stream);
+            cudaEventRecord(ev[3], g->stream);
+            cudaEventRecord(ev[4], g->stream);
+        }
+        return 0;
     }
     if (mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0) {
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,

@@ -181,3 +181,37 @@ extern "C" int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq) {
     memcpy(out, g->graph_stats.data(), (size_t)n * 16);
     return n;
 }
+
+extern "C" int pv_last_sparse(const FvGpuIndex *g) { return g ? g->last_sparse : 0; }
+
+extern "C" int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep) {
+    if (!g || epi < 0 || epi > 2 || ns < 0 || ns > 8 || grow < 0 ||
+        !(rep == 0 || rep == 1 || rep == 2 || rep == 4))
+        return -1;
+    std::lock_guard<std::mutex> lk(g->mu);
+    g->tune_epi = epi;
+    g->tune_ns = ns;
+    g->tune_grow = grow;
+    g->tune_rep = rep;
+    return 0;
+}
+
+extern "C" int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
+                               const int32_t *children, int nchildren, const double *invals,
+                               int ninvals, uint64_t *bound, char *errbuf, size_t errlen) {
+    if (!g || !bound) return -1;
+    FvGpuQueryDesc qd;
+    memset(&qd, 0, sizeof(qd));
+    qd.proot = nnodes > 0 ? 0 : -1;
+    PredBatch pb;
+    if (compile_predicates(1, &qd.proot, sizeof(FvGpuQueryDesc), nodes, nnodes, children,
+                           nchildren, invals, ninvals, g->ncols, pb, errbuf, errlen) != 0)
+        return -1;
+    if (pb.progs.empty()) {
+        *bound = g->count;
+        return 0;
+    }
+    *bound = prog_upper_bound(g, pb.insns.data() + pb.progs[0].insn0, pb.progs[0].ninsn,
+                              pb.consts.data());
+    return 0;
+}

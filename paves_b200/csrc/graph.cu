@@ -540,8 +540,7 @@ size_t graph_smem_bytes(int dpad) {
 
 cudaError_t launch_graph(const GraphArgs &a, int nq, cudaStream_t st) {
     const size_t smem = graph_smem_bytes(a.dpad);
-    cudaError_t e =
-        cudaFuncSetAttribute(graph_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_smem_limit((const void *)graph_kernel, smem);
     if (e != cudaSuccess) return e;
     graph_kernel<<<nq, G_THREADS, smem, st>>>(a);
     return cudaGetLastError();

@@ -20,9 +20,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "index.h"
+#include "pv_internal.h"
 
 namespace pv {
 
@@ -147,6 +150,24 @@ bool pv_bf16_exact(int dim, float row_amax, float q_amax) {
 
 namespace pv {
 
+// The dynamic shared-memory limit is a per-function, per-device attribute
+// that every launch must fit, including kernel nodes of CUDA graphs captured
+// earlier. Launch sites therefore only ever raise it: a graph captured with
+// a large size stays launchable after a later call asks for a smaller one.
+cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &cur = limit[{fn, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 }  // namespace pv
 
 using namespace pv;
@@ -179,7 +200,7 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
     }
     Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
                    &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
-                   &g->scan.out_d, &g->scan.out_h, &g->graph.visited, &g->graph.res,
+                   &g->scan.out_d, &g->scan.out_h, &g->scan.sparse, &g->graph.visited, &g->graph.res,
                    &g->graph.stats, &g->graph.route, &g->graph.route_h, &g->graph.gout};
     for (Buf *b : bufs) b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -266,6 +287,7 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         if ((e = cudaMemcpy(g->d_prows, post_rows, count * (size_t)ncols * 4,
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("postings copy", e);
+        pv::build_sorted_cols(g, cols, post_rows);
     }
 
     if (l0) {
@@ -355,6 +377,7 @@ FvGpuIndex *index_view(const FvGpuIndex *g) {
     v->d_vscale = g->d_vscale;
     v->d_norm = g->d_norm;
     v->row_amax = g->row_amax;
+    v->sorted_cols = g->sorted_cols;
     v->sm_count = g->sm_count;
     v->view = true;
     if (cudaSetDevice(v->device) != cudaSuccess ||

@@ -59,6 +59,7 @@ struct ScanScratch {
     Buf cand;            // reduced-precision candidate superset keys
     Buf out_d;           // FvHit [nq][topb] + cnt [nq] + trunc [nq]
     Buf out_h{true};
+    Buf sparse;          // selective filters: row count, row ids, no-filter programs
 };
 
 struct GraphScratch {
@@ -114,10 +115,14 @@ struct FvGpuIndex {
     int last_uncertain = 0;  // queries of the last call re-run exactly (or flagged)
     // tensor-core scan shape overrides (0 = built-in choice): epilogue warp
     // groups, pipeline stages, CTAs along the rows per query tile
-    int tune_epi = 0, tune_ns = 0, tune_grow = 0;
+    int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0;
     bool view = false;  // shares another handle's device data, owns only scratch
     int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels
     int launches = 0;  // kernels launched by the last call (all iterations)
     std::vector<uint32_t> graph_stats;  // last graph batch: [nq][4] counters
+    // host copy of each attribute column's non-NaN values, ascending: bounds
+    // a filter's matches by binary search (sparse routing)
+    std::vector<std::vector<double>> sorted_cols;
+    int last_sparse = 0;  // the last brute batch took the sparse route
 };

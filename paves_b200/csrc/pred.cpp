@@ -7,6 +7,7 @@
 // re-serialized in post-order with n-ary AND/OR folded into binary steps so
 // the device evaluates it with a 64-bit bit stack. Identical predicates in a
 // batch share one program (and therefore one bitmap).
+#include <math.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -109,6 +110,129 @@ struct Walker {
     }
 };
 
+// ---- range form: a program that is an AND of comparisons and IN lists
+// becomes one PV_NODE_RANGE instruction (see common.cuh). Comparisons on
+// one column merge into one interval; IN lists of integers in [0, 64)
+// become a bit mask; anything else (OR, NOT, NE, other IN lists) keeps the
+// stack program.
+struct Term {
+    int col;
+    bool mask;
+    uint64_t bits;
+    double lo, hi;
+    bool lo_open, hi_open;
+};
+
+bool small_int(double v) { return v >= 0.0 && v < 64.0 && (double)(int)v == v; }
+
+bool to_range(const std::vector<PredInsn> &prog, const std::vector<double> &consts,
+              std::vector<PredInsn> &out, std::vector<double> &outc) {
+    struct Conj {
+        bool ok;
+        std::vector<Term> t;
+    };
+    const double inf = HUGE_VAL;
+    std::vector<Conj> st;
+    for (const PredInsn &in : prog) {
+        switch (in.kind) {
+            case FV_NODE_CMP: {
+                Term t{in.col, false, 0, -inf, inf, false, false};
+                const double c = in.value;
+                switch (in.op) {
+                    case FV_CMP_LT: t.hi = c; t.hi_open = true; break;
+                    case FV_CMP_LE: t.hi = c; break;
+                    case FV_CMP_GT: t.lo = c; t.lo_open = true; break;
+                    case FV_CMP_GE: t.lo = c; break;
+                    case FV_CMP_EQ: t.lo = c; t.hi = c; break;
+                    default: return false;  // NE is true for no NaN but not an interval
+                }
+                st.push_back({true, {t}});
+                break;
+            }
+            case FV_NODE_IN: {
+                Term t{in.col, true, 0, 0.0, 0.0, false, false};
+                bool all_small = true;
+                for (int j = 0; j < in.n; j++) {
+                    const double v = consts[in.val0 + j];
+                    if (small_int(v)) t.bits |= 1ull << (int)v;
+                    else all_small = false;
+                }
+                if (!all_small) {
+                    // one distinct value is an interval [v, v]
+                    bool same = in.n > 0;
+                    for (int j = 1; j < in.n && same; j++)
+                        same = consts[in.val0 + j] == consts[in.val0];
+                    if (!same) return false;
+                    const double v = consts[in.val0];
+                    t = Term{in.col, false, 0, v, v, false, false};
+                }
+                st.push_back({true, {t}});
+                break;
+            }
+            case FV_NODE_AND:
+                if (in.n == 0) {
+                    st.push_back({true, {}});
+                } else {
+                    if (st.size() < 2) return false;
+                    Conj b = st.back();
+                    st.pop_back();
+                    Conj &a = st.back();
+                    a.ok = a.ok && b.ok;
+                    a.t.insert(a.t.end(), b.t.begin(), b.t.end());
+                }
+                break;
+            default:
+                return false;  // OR, NOT
+        }
+    }
+    if (st.size() != 1 || !st[0].ok) return false;
+    // merge per column: one interval and one mask at most
+    std::vector<Term> terms;
+    for (const Term &t : st[0].t) {
+        Term *m = nullptr;
+        for (Term &u : terms)
+            if (u.col == t.col && u.mask == t.mask) m = &u;
+        if (!m) {
+            terms.push_back(t);
+            continue;
+        }
+        if (t.mask) {
+            m->bits &= t.bits;
+            continue;
+        }
+        if (t.lo != t.lo || m->lo != m->lo || t.hi != t.hi || m->hi != m->hi) {
+            m->lo = m->hi = NAN;  // a NaN bound fails every row
+            continue;
+        }
+        if (t.lo > m->lo) { m->lo = t.lo; m->lo_open = t.lo_open; }
+        else if (t.lo == m->lo) m->lo_open = m->lo_open || t.lo_open;
+        if (t.hi < m->hi) { m->hi = t.hi; m->hi_open = t.hi_open; }
+        else if (t.hi == m->hi) m->hi_open = m->hi_open || t.hi_open;
+    }
+    if ((int)terms.size() > PV_RANGE_MAX_TERMS) return false;
+    PredInsn r;
+    memset(&r, 0, sizeof(r));
+    r.kind = PV_NODE_RANGE;
+    r.n = (int32_t)terms.size();
+    r.val0 = 0;
+    out.assign(1, r);
+    outc.clear();
+    for (const Term &t : terms) {
+        const int meta = t.col | (t.mask ? PV_TERM_MASK : 0) | (t.lo_open ? PV_TERM_LO_OPEN : 0) |
+                         (t.hi_open ? PV_TERM_HI_OPEN : 0);
+        outc.push_back((double)meta);
+        if (t.mask) {
+            double b;
+            memcpy(&b, &t.bits, 8);
+            outc.push_back(b);
+        } else {
+            outc.push_back(t.lo);
+            outc.push_back(t.hi);
+        }
+    }
+    return true;
+}
+
 }  // namespace
 
 // Compiles the per-query predicates of a batch. Returns 0, or -1 + errbuf.
@@ -151,6 +275,14 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
             snprintf(errbuf, errlen, "gpu: query %d predicate needs a stack deeper than 63", q);
             return -1;
         }
+        {
+            std::vector<PredInsn> ri;
+            std::vector<double> rc;
+            if (to_range(w.out, w.consts, ri, rc)) {
+                w.out.swap(ri);
+                w.consts.swap(rc);
+            }
+        }
         // canonical bytes: instructions with constants inlined
         std::string sig;
         int32_t colmask = 0;
@@ -161,6 +293,14 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
             if (in.kind == FV_NODE_IN)
                 sig.append((const char *)&w.consts[in.val0], sizeof(double) * in.n);
             if (in.kind == FV_NODE_CMP || in.kind == FV_NODE_IN) colmask |= (int32_t)(1u << (in.col & 31));
+            if (in.kind == PV_NODE_RANGE) {
+                sig.append((const char *)w.consts.data(), sizeof(double) * w.consts.size());
+                for (size_t j = 0, k = 0; k < (size_t)in.n; k++) {
+                    const int meta = (int)w.consts[j];
+                    colmask |= (int32_t)(1u << ((meta & 0xFFFF) & 31));
+                    j += (meta & PV_TERM_MASK) ? 2 : 3;
+                }
+            }
         }
         auto it = seen.find(sig);
         int pid;
@@ -173,7 +313,7 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
             pg.ninsn = (int32_t)w.out.size();
             int32_t cbase = (int32_t)pb.consts.size();
             for (PredInsn in : w.out) {
-                if (in.kind == FV_NODE_IN) in.val0 += cbase;
+                if (in.kind == FV_NODE_IN || in.kind == PV_NODE_RANGE) in.val0 += cbase;
                 pb.insns.push_back(in);
             }
             pb.consts.insert(pb.consts.end(), w.consts.begin(), w.consts.end());

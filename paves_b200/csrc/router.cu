@@ -41,11 +41,11 @@ constexpr int P_N = P_B3 + NO;
 static_assert(P_N == PV_MLP_NPARAMS, "parameter layout");
 
 // ---------------------------------------------------------------- features
-// One CTA per query; warp w scores centroids w, w+8, ... with lanes across
-// dimensions and keeps a sorted top-8 per lane; each warp reduces its
-// lanes' lists to a top-8 by 8 rounds of warp-wide minimum, and warp 0 does
-// the same over the 8 warps' lists. Under 1 KB of shared memory, so the
-// kernel can run beside a scan that holds most of each SM's.
+// One CTA per query; each thread scores its share of the centroids (four
+// rows at a time) and keeps a sorted top-8; each warp reduces its lanes'
+// lists to a top-8 by 8 rounds of warp-wide minimum, and warp 0 does the
+// same over the 8 warps' lists. Under 1 KB of shared memory, so the kernel
+// can run beside a scan that holds most of each SM's.
 __device__ __forceinline__ float pick8(const float (&t)[8], int i) {
     float v = INFINITY;
 #pragma unroll
@@ -84,23 +84,33 @@ __global__ void __launch_bounds__(256) router_features_kernel(
         for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) s_norm = sqrtf(s);
     }
+    // thread-per-centroid: each thread walks whole centroid rows (several
+    // rows' loads in flight), keeping its sorted top-8
     float top[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) top[i] = INFINITY;
-    for (int c = warp; c < ncent; c += 8) {
-        const float *x = cent + (uint64_t)c * dpad;
-        float acc = 0.f;
-        for (int j = lane * 4; j < dpad; j += 128) {
-            const float4 v = __ldg((const float4 *)(x + j));
-            const float4 w = *(const float4 *)(sq + j);
-            const float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
-            acc = fmaf(d0, d0, acc); acc = fmaf(d1, d1, acc);
-            acc = fmaf(d2, d2, acc); acc = fmaf(d3, d3, acc);
+    for (int c0 = tid; c0 < ncent; c0 += 4 * blockDim.x) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        const float *x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int c = c0 + u * blockDim.x;
+            x[u] = cent + (uint64_t)(c < ncent ? c : c0) * dpad;
         }
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        // lane (c / 8) % 32 keeps centroid c
-        if (lane == ((c >> 3) & 31) && acc < top[7]) {
-            float v = acc;
+        for (int j = 0; j < dpad; j += 4) {
+            const float4 w = *(const float4 *)(sq + j);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float4 v = __ldg((const float4 *)(x[u] + j));
+                const float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
+                acc[u] = fmaf(d0, d0, acc[u]); acc[u] = fmaf(d1, d1, acc[u]);
+                acc[u] = fmaf(d2, d2, acc[u]); acc[u] = fmaf(d3, d3, acc[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (c0 + u * (int)blockDim.x >= ncent || !(acc[u] < top[7])) continue;
+            float v = acc[u];
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const float t = top[i];
@@ -523,8 +533,7 @@ cudaError_t launch_router_features(const PvRouter *r, const float *d_q, int dpad
                                    float *feats, cudaStream_t st) {
     if (dpad != r->dpad) return cudaErrorInvalidValue;
     const size_t smem = router_features_smem(dpad);
-    cudaError_t e = cudaFuncSetAttribute(router_features_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_smem_limit((const void *)router_features_kernel, smem);
     if (e != cudaSuccess) return e;
     router_features_kernel<<<nq, 256, smem, st>>>(d_q, dpad, r->d_cent, r->ncent, popcnt, qprog,
                                                   nrows, kq, kind, feats);

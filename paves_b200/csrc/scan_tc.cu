@@ -21,8 +21,14 @@
 // rows (the benchmark data) every distance is exact; FP8-E4M3 rows carry a
 // per-row scale (absmax / 448) and the query a per-query scale.
 //
-// Warp roles (192 threads): warp 0 TMA producer, warp 1 TMEM allocator +
-// MMA issuer, warps 2-5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).
+// Warp roles (64 + 128 * EPI threads): warp 0 TMA producer, warp 1 TMEM
+// allocator + MMA issuer, then EPI groups of 4 epilogue warps (warp w reads
+// TMEM lanes 32*(w%4)..+31; group h takes its share of each tile's rows).
+// A batch of at most 64 (32) queries is replicated 2 (4) times down the
+// 128 query slots of the A tile: the MMA costs the same, and each replica
+// takes a disjoint share of every tile's rows, so the epilogue work per
+// warp shrinks by the replication factor and all four SM sub-partitions
+// work (without it the warps of the padding lanes idle).
 // All waits are bounded by a deadline and unwind through an abort flag.
 #include <algorithm>
 
@@ -68,7 +74,9 @@ struct TcArgs {
     uint64_t tiles_per_cta;
     uint64_t tile0_mul;  // first tile of CTA group g = g * tile0_mul
     uint64_t tile_step;  // stride between a CTA's tiles
-    int KP;             // list length per (query, CTA half)
+    int KP;             // list length per (query, CTA part)
+    int rep;            // query replicas down the tile's 128 slots (1, 2, 4)
+    int bq;             // query slots per replica = TC_BM / rep
     int push_tau;       // a full list's last key bounds the superset (lists hold it all)
     int NS;             // pipeline stages
     const float *__restrict__ xnorm;   // [rows padded to 128]
@@ -79,8 +87,14 @@ struct TcArgs {
     const uint32_t *__restrict__ bitmaps;
     uint64_t bm_words;
     unsigned long long *tau;  // [nq] grid-wide bound
-    uint64_t *part;           // [nq][grow][KP]
-    uint32_t *part_cnt;       // [nq][grow]
+    // kept keys: each list appends its best kwrite keys to its query's dense
+    // run dense[q][0 .. dcnt[q]) (any order; dcap >= lists per query * kwrite)
+    uint64_t *dense;
+    uint32_t *dcnt;
+    uint64_t dcap;
+    int kwrite;
+    // [nq] smallest last key of a full list (the merge's certificate), or null
+    unsigned long long *fullmin;
     int *err;
     uint64_t timeout_ns;
     // optional per-tile timestamps of CTA 0 (globaltimer ns):
@@ -235,15 +249,20 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------ epilogue
-        // EPI warps per TMEM lane quadrant: warp w serves the queries of lanes
-        // 32*(w%4).. and the row half (w-2)/4 of every tile.
-        constexpr int CPH = 4 / EPI;         // 32-row chunks per half
+        // EPI warps per TMEM lane quadrant: warp w serves the query slots of
+        // lanes 32*(w%4).. (replica m / bq of query m % bq) and, of every
+        // tile, the CW rows of part (half, replica).
+        constexpr int CPH = 4 / EPI;         // 32-row chunks per half at most
         constexpr int NSLOT = TC_BM * EPI;   // list / stage slots
         const int qd = warp & 3;
         const int half = (warp - 2) >> 2;
-        const int m = qd * 32 + lane;        // query slot within the tile
+        const int m = qd * 32 + lane;        // TMEM lane = query slot of the tile
+        const int rp = m / a.bq;             // replica (uniform within a warp)
         const int slot = half * TC_BM + m;
-        const int qg = qtile * TC_BM + m;
+        const int qg = qtile * TC_BM + (m - rp * a.bq);
+        const int CW = TC_BN / (EPI * a.rep);  // rows of a tile per part (>= 32)
+        const int nch = CW / 32;
+        const int col0 = (half * a.rep + rp) * CW;
         const bool qvalid = qg < a.nq;
         const float qn = qvalid ? a.qnorm[qg] : 0.f;
         const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
@@ -265,9 +284,10 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         unsigned long long gt = KEY_MAX;
         auto load_tile = [&](uint64_t tt, float (&x)[CPH], float (&s)[CPH], uint32_t (&w)[CPH],
                              unsigned long long &g) {
-            const uint64_t rb = (tile0 + tt * a.tile_step) * TC_BN + half * (TC_BN / EPI);
+            const uint64_t rb = (tile0 + tt * a.tile_step) * TC_BN + col0;
 #pragma unroll
             for (int j = 0; j < CPH; j++) {
+                if (j >= nch) break;
                 x[j] = __ldg(a.xnorm + rb + j * 32 + lane);
                 s[j] = FP8 ? __ldg(a.xscale + rb + j * 32 + lane) : 1.f;
                 const uint64_t r0 = rb + j * 32;
@@ -292,16 +312,17 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             tc_fence_after();
             const bool tr = a.trace && blockIdx.x == 0 && slot == 0 && t < (uint64_t)a.trace_tiles;
             if (tr) a.trace[t * 4 + 2] = globaltimer();
-            const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN + half * (TC_BN / EPI);
+            const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN + col0;
             if (gt < thr) {
                 thr = gt;
                 thr_d = key_dist(gt);
             }
 #pragma unroll
             for (int c = 0; c < CPH; c++) {
+                if (c >= nch) break;
                 uint32_t r[32];
                 tmem_ld_32x32b_x32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)acc * TC_BN +
-                                       half * (TC_BN / EPI) + c * 32,
+                                       col0 + c * 32,
                                    r);
                 tmem_ld_wait();
                 // hot loop: distances and a candidate mask only; the rare
@@ -408,11 +429,16 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 }
                 PV_L(j) = v;
             }
-            // partial list (rgrp, half) of query qg; the merge sees grow*EPI lists
-            const uint64_t li = (uint64_t)qg * a.grow * EPI + (uint64_t)rgrp * EPI + half;
-            uint64_t *dst = a.part + li * KP;
-            for (int i = 0; i < n; i++) dst[i] = PV_L(i);
-            a.part_cnt[li] = (uint32_t)n;
+            // the list's best kwrite keys join its query's dense run (one
+            // atomic per list); a full list reports its last key, below
+            // which it cannot have dropped anything
+            const int nw = n < a.kwrite ? n : a.kwrite;
+            if (nw > 0) {
+                const uint64_t b0 = atomicAdd(a.dcnt + qg, (uint32_t)nw);
+                uint64_t *dst = a.dense + (uint64_t)qg * a.dcap;
+                for (int i = 0; i < nw && b0 + i < a.dcap; i++) dst[b0 + i] = PV_L(i);
+            }
+            if (a.fullmin && n == KP) atomicMin(a.fullmin + qg, (unsigned long long)PV_L(KP - 1));
         }
 #undef PV_L
     }
@@ -430,21 +456,24 @@ namespace pv {
 // ---------------------------------------------------------------- queries
 // f32 queries [nq][dpad] -> low-precision tile rows [nqpad][row_bytes] with
 // zero padding, plus ||q||^2 of the rounded query (and the fp8 scale).
+// Row qi holds query qi % bq (bq = nqpad without replication).
 __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad, int dim,
-                                  int nqpad, int kelems, bool fp8, unsigned char *__restrict__ out,
-                                  float *__restrict__ qnorm, float *__restrict__ qscale) {
+                                  int nqpad, int bq, int kelems, bool fp8,
+                                  unsigned char *__restrict__ out, float *__restrict__ qnorm,
+                                  float *__restrict__ qscale) {
     const int lane = threadIdx.x & 31;
     const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (qi >= nqpad) return;
-    const bool ok = qi < nq;
+    const int src = qi % bq;
+    const bool ok = src < nq;
     float amax = 0.f;
     if (fp8 && ok)
-        for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(q[(size_t)qi * dpad + j]));
+        for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(q[(size_t)src * dpad + j]));
     for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     const float s = amax > 0.f ? amax / 448.f : 1.f;
     float acc = 0.f;
     for (int j = lane; j < kelems; j += 32) {
-        const float v = (ok && j < dim) ? q[(size_t)qi * dpad + j] : 0.f;
+        const float v = (ok && j < dim) ? q[(size_t)src * dpad + j] : 0.f;
         float r;
         if (fp8) {
             __nv_fp8_e4m3 b(v / s);
@@ -535,6 +564,196 @@ rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict_
     }
 }
 
+// ---------------------------------------------------------------- merge
+// Per-query merge of the tensor-core scan's kept keys (one CTA per query).
+// Query q's keys are dense[q][0 .. dcnt[q]) in any order; only keys at or
+// below the grid-wide bound can be in the answer. Keys are unique 64-bit
+// (distance bits, row) values, so the KO-th smallest is found exactly by a
+// radix select, 8 bits per pass (a histogram of the digit among the keys
+// that share the digits chosen so far), and only the at most KO keys at or
+// below it are sorted. Up to DM_CAP keys are staged in shared memory;
+// longer runs are read from global memory on every pass.
+constexpr int DM_THREADS = 512;
+constexpr int DM_CAP = 8192;
+constexpr int DM_OUT = TC_MAX_SUPERSET;
+
+__device__ __forceinline__ void dm_hist_add(unsigned *hist, bool act, unsigned d, int lane) {
+    const int tag = act ? (int)d : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, tag);
+    if (act && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (unsigned)__popc(peers));
+}
+
+__global__ void __launch_bounds__(DM_THREADS)
+dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *__restrict__ dcnt,
+                   int reset_cnt, const unsigned long long *__restrict__ fullmin,
+                   const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
+                   const unsigned long long *__restrict__ popcnt, uint64_t nrows,
+                   FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
+                   uint8_t *__restrict__ trunc, unsigned long long *tau_out,
+                   uint8_t *__restrict__ unc) {
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    uint64_t *buf = (uint64_t *)dm_smem;  // [DM_CAP] staged keys
+    uint64_t *res = buf + DM_CAP;         // [DM_OUT] the answer, sorted
+    __shared__ unsigned hist[256];
+    __shared__ int s_m, s_c, s_digit, s_rank, s_tot;
+    constexpr int NW = DM_THREADS / 32;
+    const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned long long bound = tau[q];
+    uint64_t n = dcnt[q];
+    if (n > dcap) n = dcap;
+    const uint64_t *src = dense + (uint64_t)q * dcap;
+    if (tid == 0) {
+        s_m = 0;
+        s_c = 0;
+    }
+    __syncthreads();
+    if (reset_cnt && tid == 0) dcnt[q] = 0;  // every thread has read it
+    const bool staged = n <= (uint64_t)DM_CAP;
+    if (staged) {
+        for (uint64_t b = (uint64_t)warp * 32; b < n; b += NW * 32) {
+            const uint64_t i = b + lane;
+            const uint64_t key = i < n ? src[i] : KEY_MAX;
+            const bool keep = i < n && key <= bound;
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            int base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&s_m, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) buf[base + __popc(bal & ((1u << lane) - 1u))] = key;
+        }
+    }
+    __syncthreads();
+    // candidates: buf[0, s_m) if staged, else the keys <= bound of src[0, n)
+    const uint64_t N = staged ? (uint64_t)s_m : n;
+    uint64_t kth = KEY_MAX;  // keep every candidate unless there are more than KO
+    if (!staged || s_m > KO) {
+        uint64_t prefix = 0;
+        int rank = KO;
+        bool selected = true;
+        for (int pass = 0; pass < 8; pass++) {
+            const int shift = 56 - 8 * pass;
+            for (int i = tid; i < 256; i += DM_THREADS) hist[i] = 0;
+            __syncthreads();
+            for (uint64_t b = (uint64_t)warp * 32; b < N; b += NW * 32) {
+                const uint64_t i = b + lane;
+                uint64_t key = KEY_MAX;
+                bool act = false;
+                if (i < N) {
+                    key = staged ? buf[i] : src[i];
+                    act = staged || key <= bound;
+                }
+                if (pass > 0) act = act && (key >> (shift + 8)) == (prefix >> (shift + 8));
+                dm_hist_add(hist, act, (unsigned)(key >> shift) & 255u, lane);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                unsigned c[8], sum = 0;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    c[j] = hist[lane * 8 + j];
+                    sum += c[j];
+                }
+                unsigned incl = sum;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const unsigned excl = incl - sum;
+                if (pass == 0 && lane == 31) s_tot = (int)incl;
+                if (excl < (unsigned)rank && (unsigned)rank <= incl) {
+                    unsigned cum = excl;
+                    int j = 0;
+                    for (; j < 7; j++) {
+                        if (cum + c[j] >= (unsigned)rank) break;
+                        cum += c[j];
+                    }
+                    s_digit = lane * 8 + j;
+                    s_rank = rank - (int)cum;
+                }
+            }
+            __syncthreads();
+            if (pass == 0 && s_tot <= KO) {  // no more than KO candidates
+                selected = false;
+                break;
+            }
+            prefix |= (uint64_t)s_digit << shift;
+            rank = s_rank;
+        }
+        if (selected) kth = prefix;
+    }
+    // the answer: candidates <= kth (exactly min(count, KO) keys)
+    for (uint64_t b = (uint64_t)warp * 32; b < N; b += NW * 32) {
+        const uint64_t i = b + lane;
+        uint64_t key = KEY_MAX;
+        if (i < N) key = staged ? buf[i] : src[i];
+        const bool keep = i < N && key <= bound && key <= kth;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        int base = 0;
+        if (lane == 0 && bal) base = atomicAdd(&s_c, __popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+        if (keep && pos < DM_OUT) res[pos] = key;
+    }
+    __syncthreads();
+    const int c = min(min(s_c, KO), DM_OUT);
+    int n2 = 1;
+    while (n2 < c) n2 <<= 1;
+    for (int i = c + tid; i < n2; i += DM_THREADS) res[i] = KEY_MAX;
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < (n2 >> 1); i += DM_THREADS) {
+                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                const int hi = lo | j;
+                const uint64_t x = res[lo], y = res[hi];
+                if ((x > y) == ((lo & k) == 0)) {
+                    res[lo] = y;
+                    res[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < c; i += DM_THREADS) {
+        FvHit h;
+        h.node = (uint64_t)key_row(res[i]);
+        h.dist = key_dist(res[i]);
+        out[(uint64_t)q * KO + i] = h;
+    }
+    if (tid == 0) {
+        out_cnt[q] = (uint32_t)c;
+        const int pg = qprog[q];
+        const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
+        trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
+        // the KO-th merged key bounds the KO-th key of any superset of rows
+        if (tau_out && c == KO && res[KO - 1] < tau_out[q]) tau_out[q] = res[KO - 1];
+        if (unc) {
+            // a full list whose last key is at or below the answer's last key
+            // (or the bound while the answer is short) may have dropped a
+            // member of it
+            const unsigned long long lim = c == KO ? res[KO - 1] : bound;
+            const unsigned long long fm = fullmin ? fullmin[q] : KEY_MAX;
+            unc[q] = (fm != KEY_MAX && fm <= lim) ? 1 : 0;
+        }
+    }
+}
+
+static cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,
+                                      bool reset_cnt, const unsigned long long *fullmin,
+                                      const unsigned long long *tau, int KO, const int32_t *qprog,
+                                      const unsigned long long *popcnt, uint64_t nrows, int nq,
+                                      FvHit *out, uint32_t *out_cnt, uint8_t *trunc,
+                                      unsigned long long *tau_out, uint8_t *unc,
+                                      cudaStream_t st) {
+    if (KO < 1 || KO > DM_OUT) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)(DM_CAP + DM_OUT) * 8;
+    cudaError_t e = raise_smem_limit((const void *)dense_merge_kernel, smem);
+    if (e != cudaSuccess) return e;
+    dense_merge_kernel<<<nq, DM_THREADS, smem, st>>>(dense, dcap, dcnt, reset_cnt ? 1 : 0, fullmin,
+                                                     tau, KO, qprog, popcnt, nrows, out, out_cnt,
+                                                     trunc, tau_out, unc);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- host side
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -605,7 +824,7 @@ static cudaError_t tc_launch(bool fp8, int grid, size_t smem, cudaStream_t st,
                             const CUtensorMap &tmX, const CUtensorMap &tmQ, const TcArgs &a) {
     const void *fn = fp8 ? (const void *)scan_tc_kernel<true, EPI>
                          : (const void *)scan_tc_kernel<false, EPI>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_smem_limit(fn, smem);
     if (e != cudaSuccess) return e;
     if (fp8)
         scan_tc_kernel<true, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
@@ -658,6 +877,13 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const size_t smem = tc_smem(kblocks, NS, KP, EPI);
     const int qtiles = (nq + TC_BM - 1) / TC_BM;
     const int nqpad = qtiles * TC_BM;
+    // query replicas: as many as the batch leaves room for, while each
+    // part of a tile keeps at least 32 rows (one TMEM load)
+    int R = 1;
+    if (g->tune_rep > 0) R = g->tune_rep;
+    else if (qtiles == 1) R = nq <= 32 ? 4 : nq <= 64 ? 2 : 1;
+    while (R > 1 && (TC_BM / R < nq || TC_BN / (EPI * R) < 32)) R >>= 1;
+    const int bq = TC_BM / R;
     const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;
     int grow = g->tune_grow > 0 ? g->tune_grow : g->sm_count / qtiles;
     if (grow < 1) grow = 1;
@@ -678,17 +904,26 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const size_t cbytes = off_unc + (size_t)nq + 256;
     PV_CUDA_OK(s.cand.ensure(cbytes), errbuf, errlen);
     PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
-    const int nlists = grow * EPI;  // partial lists per query
-    PV_CUDA_OK(s.part.ensure((size_t)nq * nlists * KP * 8), errbuf, errlen);
-    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * nlists * 4), errbuf, errlen);
+    const int nlists = grow * EPI * R;  // lists per query
+    const uint64_t dcap = (uint64_t)nlists * KP;  // a query's dense run at most
+    PV_CUDA_OK(s.part.ensure((size_t)nq * dcap * 8), errbuf, errlen);
+    // [dcnt u32 x nq][fullmin u64 x nq]
+    const size_t off_fm = ((size_t)nq * 4 + 255) & ~(size_t)255;
+    PV_CUDA_OK(s.part_cnt.ensure(off_fm + (size_t)nq * 8), errbuf, errlen);
+    uint32_t *d_dcnt = s.part_cnt.as<uint32_t>();
+    unsigned long long *d_fullmin = (unsigned long long *)(s.part_cnt.as<char>() + off_fm);
     unsigned char *c = s.cand.as<unsigned char>();
     int *d_err = (int *)(c + off_err);
+    const bool certify = KP < S;  // lists shorter than the superset
     PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
     PV_CUDA_OK(cudaMemsetAsync(d_err, 0, 4, g->stream), errbuf, errlen);
+    PV_CUDA_OK(cudaMemsetAsync(d_dcnt, 0, (size_t)nq * 4, g->stream), errbuf, errlen);
+    if (certify)
+        PV_CUDA_OK(cudaMemsetAsync(d_fullmin, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
 
     g->launches += 4;  // query prep, main pass, merge, re-rank
     query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
-        d_q, nq, g->dpad, g->dim, nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
+        d_q, nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
         fp8 ? (float *)(c + off_qs) : nullptr);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
 
@@ -706,6 +941,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.grow = grow;
     a.tiles_per_cta = tpc;
     a.KP = KP;
+    a.rep = R;
+    a.bq = bq;
     a.push_tau = KP == S ? 1 : 0;
     a.NS = NS;
     a.xnorm = g->d_norm;
@@ -716,8 +953,11 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.bitmaps = bitmaps;
     a.bm_words = bm_words;
     a.tau = s.tau.as<unsigned long long>();
-    a.part = s.part.as<uint64_t>();
-    a.part_cnt = s.part_cnt.as<uint32_t>();
+    a.dense = s.part.as<uint64_t>();
+    a.dcnt = d_dcnt;
+    a.dcap = dcap;
+    a.kwrite = KP;
+    a.fullmin = certify ? d_fullmin : nullptr;
     a.err = d_err;
     a.timeout_ns = 2000000000ull;
     a.trace = nullptr;
@@ -752,18 +992,17 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sa.tile0_mul = region;
         sa.tile_step = std::max<uint64_t>(1, region / m);
         sa.tiles_per_cta = m;
-        g->launches += 2;  // seeding pass + its merge
-        PV_CUDA_OK(run(sa), errbuf, errlen);
-        ScanPlan sp;
-        sp.M = 4096;
-        sp.merge_smem = (size_t)sp.M * 8 + (size_t)nlists * 8;
         // only each list's best keys: the S-th key of a subset of the
         // sample still bounds the S-th key of the scan, and the subset
-        // fits the merge buffer in one pass
-        const int kuse = std::max(1, std::min(KP, sp.M / std::max(1, nlists)));
-        PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, sp, a.tau, d_qprog, popcnt,
-                                g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream,
-                                a.tau, S, nullptr, kuse),
+        // stays within the merge's shared-memory stage
+        sa.kwrite = std::max(1, std::min(KP, DM_CAP / std::max(1, nlists)));
+        sa.fullmin = nullptr;
+        g->launches += 2;  // seeding pass + its merge
+        PV_CUDA_OK(run(sa), errbuf, errlen);
+        // the merge leaves the counts at zero for the main pass
+        PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, true, nullptr, a.tau, S, d_qprog,
+                                      popcnt, g->count, nq, cand, ccnt,
+                                      (uint8_t *)(c + off_ctr), a.tau, nullptr, g->stream),
                    errbuf, errlen);
     }
     // stage boundary: everything before the main pass (bitmaps, query prep,
@@ -773,13 +1012,10 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.tile_step = 1;
     PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
-    ScanPlan pl;
-    pl.M = 4096;
-    pl.merge_smem = (size_t)pl.M * 8 + (size_t)nlists * 8;
-    uint8_t *d_unc = KP < S ? (uint8_t *)(c + off_unc) : nullptr;
-    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, nlists, KP, pl, a.tau, d_qprog, popcnt, g->count,
-                            nq, cand, ccnt, (uint8_t *)(c + off_ctr), g->stream, nullptr, S,
-                            d_unc),
+    uint8_t *d_unc = certify ? (uint8_t *)(c + off_unc) : nullptr;
+    PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, false, a.fullmin, a.tau, S, d_qprog,
+                                  popcnt, g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr),
+                                  nullptr, d_unc, g->stream),
                errbuf, errlen);
     g->tc_unc = d_unc;
     g->tc_unc_n = nq;

@@ -135,3 +135,31 @@ def test_fp8_large_k_superset_certified_or_rerun(clustered):
         assert np.array_equal(dists[q, :c], exact)
         assert np.all(np.diff(dists[q, :c]) >= 0)
     gi.close()
+
+
+@pytest.mark.parametrize("epi,rep,nq", [(1, 4, 1), (1, 4, 24), (2, 2, 24), (1, 2, 64),
+                                        (2, 2, 64), (2, 1, 64), (1, 1, 40), (2, 4, 16)])
+def test_tc_epilogue_shapes_match_oracle(epi, rep, nq):
+    """Every epilogue shape (warp groups x query replicas down the tile)
+    returns exactly the oracle's top-k on integer rows: replicas split each
+    tile's rows, so a lost or doubly counted row would show here."""
+    from paves_b200 import _lib
+    L = _lib.lib()
+    ds = datagen.make_dataset(90_001, 128, nq=nq)
+    gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_BF16)
+    assert L.pv_tc_shape(gi.handle, epi, 0, 0, rep) == 0
+    six = list(datagen.six_predicates().values()) + [None]
+    preds = [six[(q + 3) % len(six)] for q in range(nq)]
+    bp = pred.concat(preds, len(ds.vectors))
+    for topb in (1, 10):
+        ids, dists, cnt, trunc = gi.brute_batch_raw(ds.queries, bp, topb)
+        assert L.pv_last_sparse(gi.handle) == 0 and L.pv_last_superset(gi.handle) > 0
+        o_ids, _, o_d32, o_cnt, o_pass = cpu.exact_topk(ds.vectors, ds.cols, ds.queries, bp, topb)
+        for q in range(nq):
+            n = int(o_cnt[q])
+            assert cnt[q] == n, (q, topb)
+            assert np.array_equal(ids[q, :n], o_ids[q, :n].astype(np.uint64)), (q, topb)
+            assert np.array_equal(dists[q, :n], o_d32[q, :n]), (q, topb)
+            assert trunc[q] == (o_pass[q] > topb)
+    assert L.pv_tc_shape(gi.handle, 0, 0, 0, 3) == -1
+    gi.close()

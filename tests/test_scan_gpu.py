@@ -175,3 +175,93 @@ def test_prepared_batch_matches_abi(golden_index, brute_golden):
     ids, dists, cnt2, tr2 = golden_index.brute_batch_raw(q, bp, 10)
     assert np.array_equal(out["node"].reshape(nq, 10), ids)
     assert np.array_equal(cnt, cnt2) and np.array_equal(tr, tr2)
+
+
+def _bound(g, p):
+    import ctypes as C
+    from paves_b200 import _lib
+    s = pred.serialize(p)
+    b = C.c_uint64()
+    err = C.create_string_buffer(256)
+    rc = _lib.lib().pv_filter_bound(g.handle, _lib.ptr(s.nodes), len(s.nodes),
+                                    _lib.ptr(s.children), len(s.children), _lib.ptr(s.invals),
+                                    len(s.invals), C.byref(b), err, 256)
+    assert rc == 0, err.value
+    return int(b.value)
+
+
+def test_selective_filters_take_the_sparse_route():
+    """A batch sharing one selective filter scans only its matching rows
+    (bitmap -> row list -> exact scan of the list); results equal the
+    oracle's, and the host bound on matches never falls below the truth,
+    including NaN attributes, NE, NOT, OR and duplicate IN values."""
+    from paves_b200 import _lib
+    rng = np.random.default_rng(11)
+    n = 120_000
+    ds = datagen.make_dataset(n, 64, nq=40)
+    cols = ds.cols.copy()
+    cols[1, rng.choice(n, 500, replace=False)] = np.nan
+    g = GpuIndex(ds.vectors, cols)
+    P, Cc = datagen.COL_PRICE, datagen.COL_CATEGORY
+    preds = [pred.Cmp(P, "<", 5.0), pred.And(pred.Cmp(P, "<", 50.0), pred.In(Cc, [3.0, 3.0])),
+             pred.Cmp(P, "==", float(cols[1][7])), pred.Not(pred.Cmp(P, ">=", 3.0)),
+             pred.Or(pred.Cmp(P, "<", 2.0), pred.Cmp(P, ">", 998.0)),
+             pred.And(pred.Cmp(P, "!=", 500.0), pred.Cmp(P, "<", 30.0)),
+             pred.Cmp(P, "<", 600.0), pred.In(Cc, [1.0, 2.0])]
+    routes = []
+    for p in preds:
+        truth = int(pred.eval_numpy(p, cols).sum())
+        assert _bound(g, p) >= truth, p
+        for topb in (1, 10, 300):
+            ids, dists, cnt, trunc = g.brute_batch(ds.queries, [p] * 40, topb)
+            routes.append(_lib.lib().pv_last_sparse(g.handle))
+            bp = pred.concat([p] * 40, n)
+            o = cpu.exact_topk(ds.vectors, cols, ds.queries, bp, topb)
+            check_exact(ids, dists, cnt, trunc, o[0], o[2], o[3], o[4], topb)
+    assert sum(routes) >= 15 and min(routes) == 0  # selective ones sparse, broad ones dense
+    g.close()
+
+
+def test_range_form_edge_values():
+    """Programs that are ANDs of comparisons and IN lists run in range form
+    (per-column intervals, small-integer sets); the rest on the bit-stack
+    interpreter. Both in one batch (one predicate per query, several
+    program chunks), over attributes holding NaN, +-inf, -0.0, half
+    integers and the 63/64 set boundary, against the oracle's match sets;
+    the host bound never falls below the oracle's count."""
+    rng = np.random.default_rng(5)
+    n = 4000
+    ds = datagen.make_dataset(n, 16, nq=1)
+    edge0 = np.array([np.nan, np.inf, -np.inf, -0.0, 0.0, 1.0, 62.0, 63.0, 63.5, 64.0, 65.0,
+                      -1.0, 1e300, -1e300, 5e-324, 3.0, 2.9999999999999996])
+    edge1 = np.array([np.nan, -0.0, 0.0, 1.0, 2.0, 3.0, 4.0, 9.0, 63.0, 64.0, 2.5, -3.0])
+    cols = np.empty((2, n))
+    cols[0] = np.where(rng.random(n) < 0.5, rng.choice(edge0, n), rng.integers(0, 100, n))
+    cols[1] = np.where(rng.random(n) < 0.5, rng.choice(edge1, n), rng.integers(0, 10, n))
+    g = GpuIndex(ds.vectors, cols)
+    C_, I_, A_ = pred.Cmp, pred.In, pred.And
+    consts = [np.nan, np.inf, -np.inf, -0.0, 0.0, 63.0, 63.5, 64.0, 3.0]
+    preds = [C_(c, op, v) for c in (0, 1) for op in ("<", "<=", ">", ">=", "==", "!=")
+             for v in consts]
+    preds += [
+        A_(C_(0, ">=", 3.0), C_(0, "<", 64.0)), A_(C_(0, ">", 3.0), C_(0, ">=", 3.0)),
+        A_(C_(0, "<=", 63.0), C_(0, "<", 63.0)), A_(C_(0, "==", np.nan), C_(0, "<", 5.0)),
+        A_(C_(0, ">", -np.inf), C_(0, "<", np.inf)), A_(C_(0, ">=", 64.0), C_(0, "<=", 3.0)),
+        A_(I_(1, [1.0, 2.0, 3.0]), I_(1, [2.0, 3.0, 4.0])),
+        A_(I_(1, [63.0, 0.0]), C_(0, "<", 100.0)), A_(), I_(1, []), I_(1, [2.5]),
+        I_(1, [2.5, 2.5]), I_(1, [2.5, 3.0]), I_(1, [-0.0]), I_(1, [64.0]), I_(0, [np.nan]),
+        I_(0, [63.0, 64.0]), A_(A_(C_(0, ">=", 1.0), I_(1, [1.0, 9.0])),
+                                  A_(C_(0, "<=", 62.0), C_(1, "<", 9.0))),
+        A_(C_(0, ">=", 0.0), C_(0, "<=", -0.0)), A_(I_(1, [3.0]), C_(1, ">=", 3.0)),
+        pred.Or(C_(0, "<", 1.0), C_(1, "==", 2.0)), pred.Not(C_(0, "<", 3.0)),
+        A_(C_(0, "<", 50.0), pred.Not(I_(1, [2.0]))), A_(C_(0, "!=", 3.0), C_(0, "<", 10.0)),
+    ]
+    nq = len(preds)
+    q = np.repeat(ds.queries[:1], nq, axis=0)
+    ids, dists, cnt, trunc = g.brute_batch(q, preds, 4096)
+    bp = pred.concat(preds, n)
+    o = cpu.exact_topk(ds.vectors, cols, q, bp, 4096)
+    check_exact(ids, dists, cnt, trunc, o[0], o[2], o[3], o[4], 4096)
+    for i, p in enumerate(preds):
+        assert _bound(g, p) >= int(o[4][i]), p
+    g.close()

@@ -88,7 +88,9 @@ def test_tuning_file_reloads(env):
 
 def test_predicate_overflow_takes_the_ordinary_path(env):
     ds, g, s, path = env
-    big = pred.In(datagen.COL_CATEGORY, [float(c) for c in range(10)] * 10)  # 100 values
+    # 100 distinct values, not all small integers: stays a 100-constant IN list
+    big = pred.In(datagen.COL_CATEGORY, [float(c) for c in range(10)] +
+                  [100.5 + c for c in range(90)])
     q = ds.queries[:1]
     ids, dists, cnt, ms = s.run(q, [big], 10)
     assert s.last()["fallback"] == 1
