@@ -66,7 +66,9 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
         if (all) {
             const uint64_t b = prog_upper_bound(g, pb.insns.data() + pb.progs[0].insn0,
                                                 pb.progs[0].ninsn, pb.consts.data());
-            if (b <= sparse_limit(g->count)) db.sparse_bound = b;
+            // (the route holds one key per query and listed row: 128 MB at most)
+            if (b <= sparse_limit(g->count) && (uint64_t)nq * b <= (1ull << 24))
+                db.sparse_bound = b;
         }
     }
     return 0;

@@ -31,6 +31,18 @@ cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const Pred
                                   unsigned long long *popcnt, int sm_count, cudaStream_t st,
                                   int ncols = 1 << 30);
 
+// ---- per-query top-KO of dense key runs (scan_tc.cu): keys of query q are
+// dense[q][0 .. dcnt[q]) (<= dcap), at most the bound tau[q] (tau null: no
+// bound); KO <= 1024. Writes out [nq][KO] ascending, out_cnt, trunc (from
+// popcnt[qprog[q]] or nrows), tau_out[q] = min(tau_out[q], KO-th key) and
+// unc[q] (a full list's last key, fullmin[q], at or below the answer's end).
+cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,
+                               bool reset_cnt, const unsigned long long *fullmin,
+                               const unsigned long long *tau, int KO, const int32_t *qprog,
+                               const unsigned long long *popcnt, uint64_t nrows, int nq,
+                               FvHit *out, uint32_t *out_cnt, uint8_t *trunc,
+                               unsigned long long *tau_out, uint8_t *unc, cudaStream_t st);
+
 // ---- exact FP32 scan (scan_f32.cu)
 struct ScanF32Args {
     const float *__restrict__ vecs;
@@ -48,10 +60,6 @@ struct ScanF32Args {
     unsigned long long *tau;  // [nq]
     uint64_t *part;           // [nq][grow][K]
     uint32_t *part_cnt;       // [nq][grow]
-    // gathered scan (optional): row r of the scan is index row rowids[r],
-    // and only the first *nrows_dev (<= nrows) of them exist
-    const uint32_t *__restrict__ rowids = nullptr;
-    const unsigned long long *__restrict__ nrows_dev = nullptr;
 };
 
 struct ScanPlan {
@@ -63,7 +71,7 @@ struct ScanPlan {
 };
 
 int scan_f32_max_qt(int dim);
-// min_rows: rows per CTA at least (gathered scans of few rows use less)
+// min_rows: rows per CTA at least
 bool plan_scan_f32(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPlan &pl,
                    uint64_t min_rows = 2048);
 cudaError_t launch_scan_f32(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st);
@@ -107,9 +115,9 @@ int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &p
                  uint32_t topb, const uint8_t *unc, FvHit *out, uint32_t *out_cnt,
                  uint8_t *truncated, char *errbuf, size_t errlen);
 // ---- selective filters (sparse.cu)
-// Filters bounded by at most this many rows take the sparse route: the
-// exact scan of the listed rows costs less than a full scan below ~1/16
-// of the index (at 1M x 128, 64 queries: ~60 us vs ~150 us).
+// Filters bounded by at most this many rows take the sparse route: exact
+// distances of the listed rows cost less than a full scan below ~1/16 of
+// the index.
 inline uint64_t sparse_limit(uint64_t nrows) { return nrows / 16 > 4096 ? nrows / 16 : 4096; }
 void build_sorted_cols(FvGpuIndex *g, const double *cols, const uint32_t *post_rows);
 uint64_t prog_upper_bound(const FvGpuIndex *g, const PredInsn *ins, int n, const double *consts);

@@ -50,7 +50,7 @@ __device__ __forceinline__ float butterfly32(float (&p)[32], int lane) {
     return p[0];
 }
 
-template <int QT, int DCH, bool GATHER>
+template <int QT, int DCH>
 __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
     using SH = ScanShape<QT>;
     constexpr int R = SH::R;
@@ -95,10 +95,9 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
     }
     __syncthreads();
 
-    const uint64_t nrows = GATHER ? min((unsigned long long)a.nrows, *a.nrows_dev) : a.nrows;
     const uint64_t r0 = (uint64_t)rblk * a.rows_per_cta;
     uint64_t r1 = r0 + a.rows_per_cta;
-    if (r1 > nrows) r1 = nrows;
+    if (r1 > a.nrows) r1 = a.nrows;
 
     // pair owned by this lane after the butterfly
     const int my_r = lane / QT;
@@ -125,13 +124,12 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
             for (int r = 0; r < R; r++) {
                 const uint64_t row = rb + r;
                 const bool ok = row < r1;
-                const uint64_t xrow = (GATHER && ok) ? (uint64_t)__ldg(a.rowids + row) : row;
                 float4 x[DCH];
 #pragma unroll
                 for (int c = 0; c < DCH; c++) {
                     const int j = c * 128 + lane * 4;
                     x[c] = (ok && j < a.dpad)
-                               ? __ldg((const float4 *)(a.vecs + xrow * (uint64_t)a.dpad + j))
+                               ? __ldg((const float4 *)(a.vecs + row * (uint64_t)a.dpad + j))
                                : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
 #pragma unroll
@@ -154,8 +152,7 @@ __global__ void __launch_bounds__(256, 2) scan_f32_kernel(ScanF32Args a) {
             const float dist = butterfly32(p, lane);
             const uint64_t row = rb + my_r;
             if (row < r1 && my_qg < a.nq && ((pword >> (row & 31)) & 1u)) {
-                const uint32_t krow = GATHER ? __ldg(a.rowids + row) : (uint32_t)row;
-                const uint64_t key = make_key(dist, krow);
+                const uint64_t key = make_key(dist, (uint32_t)row);
                 if (key < t.tau[my_q]) {
                     const int pos = atomicAdd(&t.nb[my_q], 1);
                     t.region[(size_t)my_q * S + K + pos] = key;
@@ -460,9 +457,9 @@ bool plan_scan_f32(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPl
     return true;
 }
 
-template <int QT, int DCH, bool GATHER>
+template <int QT, int DCH>
 static cudaError_t launch_qt(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st) {
-    auto kern = scan_f32_kernel<QT, DCH, GATHER>;
+    auto kern = scan_f32_kernel<QT, DCH>;
     cudaError_t e = raise_smem_limit((const void *)kern, pl.smem);
     if (e != cudaSuccess) return e;
     unsigned grid = (unsigned)(pl.grow * pl.qtiles);
@@ -471,10 +468,8 @@ static cudaError_t launch_qt(const ScanF32Args &a, const ScanPlan &pl, cudaStrea
 }
 
 cudaError_t launch_scan_f32(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st) {
-    if ((a.rowids == nullptr) != (a.nrows_dev == nullptr)) return cudaErrorInvalidValue;
-#define PV_CASE(Q, D)                                                        \
-    if (pl.QT == Q && pl.DCH == D)                                           \
-        return a.rowids ? launch_qt<Q, D, true>(a, pl, st) : launch_qt<Q, D, false>(a, pl, st);
+#define PV_CASE(Q, D) \
+    if (pl.QT == Q && pl.DCH == D) return launch_qt<Q, D>(a, pl, st);
     PV_CASE(1, 1) PV_CASE(2, 1) PV_CASE(4, 1) PV_CASE(8, 1) PV_CASE(16, 1)
     PV_CASE(1, 2) PV_CASE(2, 2) PV_CASE(4, 2) PV_CASE(8, 2)
     PV_CASE(1, 4) PV_CASE(2, 4) PV_CASE(4, 4)

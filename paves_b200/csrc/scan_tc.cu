@@ -456,14 +456,24 @@ namespace pv {
 // ---------------------------------------------------------------- queries
 // f32 queries [nq][dpad] -> low-precision tile rows [nqpad][row_bytes] with
 // zero padding, plus ||q||^2 of the rounded query (and the fp8 scale).
-// Row qi holds query qi % bq (bq = nqpad without replication).
+// Row qi holds query qi % bq (bq = nqpad without replication). Also resets
+// the scan's per-query state for query qi < nq: bound tau (none), dense run
+// count, full-list minimum (if tracked), and the watchdog word.
 __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad, int dim,
                                   int nqpad, int bq, int kelems, bool fp8,
                                   unsigned char *__restrict__ out, float *__restrict__ qnorm,
-                                  float *__restrict__ qscale) {
+                                  float *__restrict__ qscale, unsigned long long *__restrict__ tau,
+                                  uint32_t *__restrict__ dcnt,
+                                  unsigned long long *__restrict__ fullmin, int *__restrict__ err) {
     const int lane = threadIdx.x & 31;
     const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (qi >= nqpad) return;
+    if (lane == 0 && qi < nq) {
+        tau[qi] = KEY_MAX;
+        dcnt[qi] = 0;
+        if (fullmin) fullmin[qi] = KEY_MAX;
+        if (qi == 0) *err = 0;
+    }
     const int src = qi % bq;
     const bool ok = src < nq;
     float amax = 0.f;
@@ -571,10 +581,11 @@ rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict_
 // (distance bits, row) values, so the KO-th smallest is found exactly by a
 // radix select, 8 bits per pass (a histogram of the digit among the keys
 // that share the digits chosen so far), and only the at most KO keys at or
-// below it are sorted. Up to DM_CAP keys are staged in shared memory;
-// longer runs are read from global memory on every pass.
+// below it are sorted. Runs up to stage_cap keys are staged in shared
+// memory; longer ones are read from global memory on every pass (4 loads
+// in flight per lane).
 constexpr int DM_THREADS = 512;
-constexpr int DM_CAP = 8192;
+constexpr int DM_CAP_MAX = 24576;   // largest shared-memory stage
 constexpr int DM_OUT = TC_MAX_SUPERSET;
 
 __device__ __forceinline__ void dm_hist_add(unsigned *hist, bool act, unsigned d, int lane) {
@@ -584,21 +595,22 @@ __device__ __forceinline__ void dm_hist_add(unsigned *hist, bool act, unsigned d
 }
 
 __global__ void __launch_bounds__(DM_THREADS)
-dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *__restrict__ dcnt,
-                   int reset_cnt, const unsigned long long *__restrict__ fullmin,
+dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, int stage_cap,
+                   uint32_t *__restrict__ dcnt, int reset_cnt,
+                   const unsigned long long *__restrict__ fullmin,
                    const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
                    const unsigned long long *__restrict__ popcnt, uint64_t nrows,
                    FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
                    uint8_t *__restrict__ trunc, unsigned long long *tau_out,
                    uint8_t *__restrict__ unc) {
     extern __shared__ __align__(16) unsigned char dm_smem[];
-    uint64_t *buf = (uint64_t *)dm_smem;  // [DM_CAP] staged keys
-    uint64_t *res = buf + DM_CAP;         // [DM_OUT] the answer, sorted
+    uint64_t *buf = (uint64_t *)dm_smem;  // [stage_cap] staged keys
+    uint64_t *res = buf + stage_cap;      // [DM_OUT] the answer, sorted
     __shared__ unsigned hist[256];
     __shared__ int s_m, s_c, s_digit, s_rank, s_tot;
     constexpr int NW = DM_THREADS / 32;
     const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const unsigned long long bound = tau[q];
+    const unsigned long long bound = tau ? tau[q] : KEY_MAX;
     uint64_t n = dcnt[q];
     if (n > dcap) n = dcap;
     const uint64_t *src = dense + (uint64_t)q * dcap;
@@ -608,7 +620,7 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
     }
     __syncthreads();
     if (reset_cnt && tid == 0) dcnt[q] = 0;  // every thread has read it
-    const bool staged = n <= (uint64_t)DM_CAP;
+    const bool staged = n <= (uint64_t)stage_cap;
     if (staged) {
         for (uint64_t b = (uint64_t)warp * 32; b < n; b += NW * 32) {
             const uint64_t i = b + lane;
@@ -633,16 +645,19 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
             const int shift = 56 - 8 * pass;
             for (int i = tid; i < 256; i += DM_THREADS) hist[i] = 0;
             __syncthreads();
-            for (uint64_t b = (uint64_t)warp * 32; b < N; b += NW * 32) {
-                const uint64_t i = b + lane;
-                uint64_t key = KEY_MAX;
-                bool act = false;
-                if (i < N) {
-                    key = staged ? buf[i] : src[i];
-                    act = staged || key <= bound;
+            for (uint64_t b = (uint64_t)warp * 128; b < N; b += NW * 128) {
+                uint64_t key[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const uint64_t i = b + u * 32 + lane;
+                    key[u] = i < N ? (staged ? buf[i] : src[i]) : KEY_MAX;
                 }
-                if (pass > 0) act = act && (key >> (shift + 8)) == (prefix >> (shift + 8));
-                dm_hist_add(hist, act, (unsigned)(key >> shift) & 255u, lane);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    bool act = b + u * 32 + lane < N && (staged || key[u] <= bound);
+                    if (pass > 0) act = act && (key[u] >> (shift + 8)) == (prefix >> (shift + 8));
+                    dm_hist_add(hist, act, (unsigned)(key[u] >> shift) & 255u, lane);
+                }
             }
             __syncthreads();
             if (warp == 0) {
@@ -681,17 +696,23 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
         if (selected) kth = prefix;
     }
     // the answer: candidates <= kth (exactly min(count, KO) keys)
-    for (uint64_t b = (uint64_t)warp * 32; b < N; b += NW * 32) {
-        const uint64_t i = b + lane;
-        uint64_t key = KEY_MAX;
-        if (i < N) key = staged ? buf[i] : src[i];
-        const bool keep = i < N && key <= bound && key <= kth;
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        int base = 0;
-        if (lane == 0 && bal) base = atomicAdd(&s_c, __popc(bal));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        const int pos = base + __popc(bal & ((1u << lane) - 1u));
-        if (keep && pos < DM_OUT) res[pos] = key;
+    for (uint64_t b = (uint64_t)warp * 128; b < N; b += NW * 128) {
+        uint64_t key[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t i = b + u * 32 + lane;
+            key[u] = i < N ? (staged ? buf[i] : src[i]) : KEY_MAX;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const bool keep = b + u * 32 + lane < N && key[u] <= bound && key[u] <= kth;
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            int base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&s_c, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            const int pos = base + __popc(bal & ((1u << lane) - 1u));
+            if (keep && pos < DM_OUT) res[pos] = key[u];
+        }
     }
     __syncthreads();
     const int c = min(min(s_c, KO), DM_OUT);
@@ -737,20 +758,22 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
     }
 }
 
-static cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,
-                                      bool reset_cnt, const unsigned long long *fullmin,
-                                      const unsigned long long *tau, int KO, const int32_t *qprog,
-                                      const unsigned long long *popcnt, uint64_t nrows, int nq,
-                                      FvHit *out, uint32_t *out_cnt, uint8_t *trunc,
-                                      unsigned long long *tau_out, uint8_t *unc,
-                                      cudaStream_t st) {
+cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,
+                               bool reset_cnt, const unsigned long long *fullmin,
+                               const unsigned long long *tau, int KO, const int32_t *qprog,
+                               const unsigned long long *popcnt, uint64_t nrows, int nq,
+                               FvHit *out, uint32_t *out_cnt, uint8_t *trunc,
+                               unsigned long long *tau_out, uint8_t *unc, cudaStream_t st) {
     if (KO < 1 || KO > DM_OUT) return cudaErrorInvalidValue;
-    const size_t smem = (size_t)(DM_CAP + DM_OUT) * 8;
+    // the stage holds a whole run when it can (runs never exceed dcap)
+    const int stage_cap = (int)std::min<uint64_t>(std::max<uint64_t>(dcap, 1), DM_CAP_MAX);
+    const size_t smem = (size_t)(stage_cap + DM_OUT) * 8;
     cudaError_t e = raise_smem_limit((const void *)dense_merge_kernel, smem);
     if (e != cudaSuccess) return e;
-    dense_merge_kernel<<<nq, DM_THREADS, smem, st>>>(dense, dcap, dcnt, reset_cnt ? 1 : 0, fullmin,
-                                                     tau, KO, qprog, popcnt, nrows, out, out_cnt,
-                                                     trunc, tau_out, unc);
+    dense_merge_kernel<<<nq, DM_THREADS, smem, st>>>(dense, dcap, stage_cap, dcnt,
+                                                     reset_cnt ? 1 : 0, fullmin, tau, KO, qprog,
+                                                     popcnt, nrows, out, out_cnt, trunc, tau_out,
+                                                     unc);
     return cudaGetLastError();
 }
 
@@ -915,16 +938,12 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     unsigned char *c = s.cand.as<unsigned char>();
     int *d_err = (int *)(c + off_err);
     const bool certify = KP < S;  // lists shorter than the superset
-    PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
-    PV_CUDA_OK(cudaMemsetAsync(d_err, 0, 4, g->stream), errbuf, errlen);
-    PV_CUDA_OK(cudaMemsetAsync(d_dcnt, 0, (size_t)nq * 4, g->stream), errbuf, errlen);
-    if (certify)
-        PV_CUDA_OK(cudaMemsetAsync(d_fullmin, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
 
     g->launches += 4;  // query prep, main pass, merge, re-rank
     query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
         d_q, nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
-        fp8 ? (float *)(c + off_qs) : nullptr);
+        fp8 ? (float *)(c + off_qs) : nullptr, s.tau.as<unsigned long long>(), d_dcnt,
+        certify ? d_fullmin : nullptr, d_err);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
 
     CUtensorMap tmX, tmQ;
@@ -995,7 +1014,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         // only each list's best keys: the S-th key of a subset of the
         // sample still bounds the S-th key of the scan, and the subset
         // stays within the merge's shared-memory stage
-        sa.kwrite = std::max(1, std::min(KP, DM_CAP / std::max(1, nlists)));
+        sa.kwrite = std::max(1, std::min(KP, DM_CAP_MAX / std::max(1, nlists)));
         sa.fullmin = nullptr;
         g->launches += 2;  // seeding pass + its merge
         PV_CUDA_OK(run(sa), errbuf, errlen);

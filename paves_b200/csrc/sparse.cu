@@ -9,9 +9,9 @@
 //    (from the posting rows), so a comparison or IN list is counted exactly
 //    by binary search, and AND / OR / NOT combine lower / upper bounds;
 //  * a batch whose queries share one filter bounded by a small count
-//    compacts that filter's bitmap into a row-id list on the device and
-//    runs the exact FP32 scan over the listed rows only (the scan kernel
-//    gathers rows through the list; keys keep the index's row ids).
+//    compacts that filter's bitmap into a row-id list on the device,
+//    computes the exact FP32 distance of every (query, listed row) and
+//    selects each query's top-k from those keys (a radix select).
 // Results equal the full scan's: same rows, same FP32 distances.
 #include <math.h>
 #include <string.h>
@@ -191,8 +191,64 @@ __global__ void __launch_bounds__(256) compact_kernel(const uint32_t *__restrict
     }
 }
 
-// The sparse route of brute_launch: every query uses program 0 and its
-// bound is at most `bound` rows. Exact FP32 scan over the compacted rows.
+// Exact FP32 distances of every listed row to every query of the batch:
+// keys[q][i] = (||x_rowids[i] - q||^2, rowids[i]) for i < n = min(*count,
+// cap), and dcnt[q] = n. grid (row blocks, query tiles of GD_QT); a warp
+// takes one row at a time: lane L holds dims [4L, 4L+4) of each 128-dim
+// chunk, the GD_QT partial sums are reduced with xor-shuffles.
+constexpr int GD_QT = 8;
+
+__global__ void __launch_bounds__(256)
+gather_dist_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict__ queries,
+                   int nq, const uint32_t *__restrict__ rowids,
+                   const unsigned long long *__restrict__ count, uint64_t cap,
+                   uint64_t *__restrict__ keys, uint32_t *__restrict__ dcnt) {
+    extern __shared__ __align__(16) float gd_q[];  // [GD_QT][dpad]
+    const int q0 = blockIdx.y * GD_QT;
+    const uint64_t n = min((unsigned long long)cap, *count);
+    for (int i = threadIdx.x; i < GD_QT * dpad; i += blockDim.x) {
+        const int j = i / dpad, d = i - j * dpad;
+        gd_q[i] = q0 + j < nq ? queries[(size_t)(q0 + j) * dpad + d] : 0.f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < GD_QT && q0 + (int)threadIdx.x < nq)
+        dcnt[q0 + threadIdx.x] = (uint32_t)n;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < n; r += (uint64_t)gridDim.x * 8) {
+        const uint32_t row = __ldg(rowids + r);
+        const float *x = vecs + (uint64_t)row * dpad;
+        float acc[GD_QT];
+#pragma unroll
+        for (int j = 0; j < GD_QT; j++) acc[j] = 0.f;
+        for (int c = lane * 4; c < dpad; c += 128) {
+            const float4 v = __ldg((const float4 *)(x + c));
+#pragma unroll
+            for (int j = 0; j < GD_QT; j++) {
+                const float4 w = *(const float4 *)(gd_q + j * dpad + c);
+                const float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
+                acc[j] = fmaf(d0, d0, acc[j]);
+                acc[j] = fmaf(d1, d1, acc[j]);
+                acc[j] = fmaf(d2, d2, acc[j]);
+                acc[j] = fmaf(d3, d3, acc[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < GD_QT; j++)
+#pragma unroll
+            for (int o = 16; o; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+        float mine = acc[0];
+#pragma unroll
+        for (int j = 1; j < GD_QT; j++)
+            if (lane == j) mine = acc[j];
+        if (lane < GD_QT && q0 + lane < nq)
+            keys[(uint64_t)(q0 + lane) * cap + r] = make_key(mine, row);
+    }
+}
+
+// The sparse route of brute_launch: every query uses program 0, whose
+// matches are at most `bound` rows. The bitmap is compacted to a row list,
+// every (query, listed row) gets its exact FP32 key, and each query's
+// top-topb is selected from its keys (launch_dense_merge).
 int sparse_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, FvHit *d_out,
                   uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen) {
     const int nq = db.nq;
@@ -202,56 +258,35 @@ int sparse_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, Fv
     const uint64_t bm_words = (g->count + 31) / 32;
     ScanScratch &s = g->scan;
     const uint64_t cap = std::max<uint64_t>(bound, 1);
-    ScanPlan pl;
-    // few rows: short streams per CTA, so that the grid still fills the GPU
-    if (!plan_scan_f32(cap, g->dpad, nq, (int)topb, g->sm_count, pl, 128)) {
-        snprintf(errbuf, errlen, "gpu: dimension %d not supported by the scan", g->dim);
-        return -1;
-    }
-    // scratch: [count u64][ids u32 cap][qprog -1 x nq]
-    const size_t off_ids = 256, off_neg = off_ids + ((cap * 4 + 255) & ~(size_t)255);
-    PV_CUDA_OK(s.sparse.ensure(off_neg + (size_t)nq * 4 + 256), errbuf, errlen);
+    // scratch: [count u64][dcnt u32 x nq][ids u32 x cap][keys u64 x nq x cap]
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t off_dcnt = 256, off_ids = off_dcnt + al((size_t)nq * 4);
+    const size_t off_keys = off_ids + al(cap * 4);
+    PV_CUDA_OK(s.sparse.ensure(off_keys + (size_t)nq * cap * 8 + 256), errbuf, errlen);
     char *sp = s.sparse.as<char>();
     unsigned long long *d_count = (unsigned long long *)sp;
+    uint32_t *dcnt = (uint32_t *)(sp + off_dcnt);
     uint32_t *ids = (uint32_t *)(sp + off_ids);
-    int32_t *neg = (int32_t *)(sp + off_neg);
+    uint64_t *keys = (uint64_t *)(sp + off_keys);
     PV_CUDA_OK(cudaMemsetAsync(d_count, 0, 8, g->stream), errbuf, errlen);
-    PV_CUDA_OK(cudaMemsetAsync(neg, 0xFF, (size_t)nq * 4, g->stream), errbuf, errlen);
     unsigned blocks = (unsigned)std::min<uint64_t>((bm_words + 255) / 256, (uint64_t)g->sm_count * 4);
     if (!blocks) blocks = 1;
     compact_kernel<<<blocks, 256, 0, g->stream>>>(s.bitmaps.as<uint32_t>(), bm_words, g->count,
                                                   ids, d_count, cap);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
-    PV_CUDA_OK(s.tau.ensure((size_t)nq * 8), errbuf, errlen);
-    PV_CUDA_OK(s.part.ensure((size_t)nq * pl.grow * topb * 8), errbuf, errlen);
-    PV_CUDA_OK(s.part_cnt.ensure((size_t)nq * pl.grow * 4), errbuf, errlen);
-    PV_CUDA_OK(cudaMemsetAsync(s.tau.p, 0xFF, (size_t)nq * 8, g->stream), errbuf, errlen);
-    ScanF32Args a;
-    a.vecs = g->d_vecs;
-    a.nrows = cap;
-    a.dpad = g->dpad;
-    a.queries = d_q;
-    a.nq = nq;
-    a.bitmaps = s.bitmaps.as<uint32_t>();
-    a.bm_words = bm_words;
-    a.qprog = neg;  // every listed row passes
-    a.K = (int)topb;
-    a.S = pl.S;
-    a.CB = pl.CB;
-    a.rows_per_cta = pl.rows_per_cta;
-    a.grow = pl.grow;
-    a.qtiles = pl.qtiles;
-    a.tau = s.tau.as<unsigned long long>();
-    a.part = s.part.as<uint64_t>();
-    a.part_cnt = s.part_cnt.as<uint32_t>();
-    a.rowids = ids;
-    a.nrows_dev = d_count;
-    g->launches += 3;  // compaction, scan, merge
-    PV_CUDA_OK(launch_scan_f32(a, pl, g->stream), errbuf, errlen);
-    // the merge's truncation flag counts the filter's true matches
-    PV_CUDA_OK(launch_merge(a.part, a.part_cnt, pl.grow, (int)topb, pl, a.tau, d_qprog,
-                            s.popcnt.as<unsigned long long>(), g->count, nq, d_out, d_cnt,
-                            d_trunc, g->stream),
+    const int qtiles = (nq + GD_QT - 1) / GD_QT;
+    const uint64_t bx = std::max<uint64_t>(
+        1, std::min<uint64_t>((cap + 63) / 64, std::max(1, 4 * g->sm_count / qtiles)));
+    const size_t smem = (size_t)GD_QT * g->dpad * 4;
+    PV_CUDA_OK(raise_smem_limit((const void *)gather_dist_kernel, smem), errbuf, errlen);
+    gather_dist_kernel<<<dim3((unsigned)bx, (unsigned)qtiles), 256, smem, g->stream>>>(
+        g->d_vecs, g->dpad, d_q, nq, ids, d_count, cap, keys, dcnt);
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    g->launches += 3;  // compaction, distances, selection
+    // the truncation flag counts the filter's true matches
+    PV_CUDA_OK(launch_dense_merge(keys, cap, dcnt, false, nullptr, nullptr, (int)topb, d_qprog,
+                                  s.popcnt.as<unsigned long long>(), g->count, nq, d_out, d_cnt,
+                                  d_trunc, nullptr, nullptr, g->stream),
                errbuf, errlen);
     return 0;
 }
