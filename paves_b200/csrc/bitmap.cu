@@ -31,7 +31,7 @@ constexpr int BM_REG_COLS = 4;    // columns held in registers per row group
 constexpr int BM_PCH = 8;         // programs per work item
 constexpr int BM_INS_WIN = 256;   // a work item's instructions kept in shared memory
 constexpr int BM_CONST_WIN = 256; // constants kept in shared memory
-constexpr int BM_BLOCKS_PER_SM = 3;
+constexpr int BM_BLOCKS_PER_SM = 2;
 
 // All programs of a batch in one launch. Work items are (program chunk of
 // BM_PCH programs, row block); items of the same row block sit next to each
@@ -57,6 +57,12 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
     __shared__ double s_const[BM_CONST_WIN];
     __shared__ PredProg s_prog[BM_PCH];
     __shared__ unsigned int s_cnt[BM_PCH];
+    // range programs of the chunk, decoded: s_nt terms (-1: stack program)
+    __shared__ int s_nt[BM_PCH];
+    __shared__ int s_tcol[BM_PCH][PV_RANGE_MAX_TERMS];  // col | PV_TERM_MASK
+    __shared__ double s_tlo[BM_PCH][PV_RANGE_MAX_TERMS], s_thi[BM_PCH][PV_RANGE_MAX_TERMS];
+    __shared__ unsigned long long s_tbits[BM_PCH][PV_RANGE_MAX_TERMS];
+    __shared__ int s_mcols;  // register columns that IN-set terms test
     if (dcounts) {
         P = min(P, dcounts[0]);
         ninsns = min(ninsns, dcounts[1]);
@@ -99,8 +105,50 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
             s_prog[threadIdx.x] = pg;
             s_cnt[threadIdx.x] = 0;
         }
+        if (threadIdx.x == 0) s_mcols = 0;
         __syncthreads();
         const PredInsn *ins = ins_sm ? s_ins : insns;
+        if (threadIdx.x < BM_PCH) {
+            // decode a range program's terms; a term whose constants lie
+            // outside the batch's pool admits nothing
+            const int p = threadIdx.x;
+            const PredProg pg = s_prog[p];
+            int nt = -1;
+            if (p < np && pg.ninsn == 1 && ins[pg.insn0].kind == PV_NODE_RANGE) {
+                const PredInsn r = ins[pg.insn0];
+                nt = min(max(r.n, 0), PV_RANGE_MAX_TERMS);
+                int ci = r.val0;
+                for (int k = 0; k < nt; k++) {
+                    int tc = 0;
+                    double tlo = NAN, thi = NAN;
+                    unsigned long long bits = 0;
+                    if (ci >= 0 && ci + 2 <= nconsts) {
+                        const int meta = (int)cst[ci];
+                        const int col = meta & 0xFFFF;
+                        if (meta & PV_TERM_MASK) {
+                            tc = col | PV_TERM_MASK;
+                            bits = (unsigned long long)__double_as_longlong(cst[ci + 1]);
+                            if (col < BM_REG_COLS) atomicOr(&s_mcols, 1 << col);
+                            ci += 2;
+                        } else {
+                            tc = col;
+                            if (ci + 3 <= nconsts) {
+                                tlo = cst[ci + 1];
+                                thi = cst[ci + 2];
+                            }
+                            ci += 3;
+                        }
+                    }
+                    s_tcol[p][k] = tc;
+                    s_tlo[p][k] = tlo;
+                    s_thi[p][k] = thi;
+                    s_tbits[p][k] = bits;
+                }
+            }
+            s_nt[p] = nt;
+        }
+        __syncthreads();
+        const int mcols = s_mcols;
         const uint64_t gw = rb * (blockDim.x / 32) + (threadIdx.x >> 5);
         const uint64_t nw = nrb * (blockDim.x / 32);
         for (uint64_t grp = gw; grp < groups; grp += nw) {
@@ -140,57 +188,91 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                     for (int j = 0; j < 4; j++) v[j] = live[j] ? __ldg(c + row[j]) : 0.0;
                 }
             };
-            for (int p = 0; p < np; p++) {
-                const PredProg pg = s_prog[p];
-                if (pg.ninsn == 1 && ins[pg.insn0].kind == PV_NODE_RANGE) {
-                    // range form: AND of interval / small-integer-set terms
-                    const PredInsn r = ins[pg.insn0];
-                    bool ok[4] = {true, true, true, true};
-                    int ci = r.val0;
-                    for (int k = 0; k < r.n; k++) {
-                        if (ci < 0 || ci + 2 > nconsts) {
-                            ok[0] = ok[1] = ok[2] = ok[3] = false;
-                            break;
-                        }
-                        const int meta = (int)cst[ci];
-                        const bool is_mask = meta & PV_TERM_MASK;
-                        if (!is_mask && ci + 3 > nconsts) {
-                            ok[0] = ok[1] = ok[2] = ok[3] = false;
-                            break;
-                        }
-                        double v[4];
-                        colval(meta & 0xFFFF, v);
-                        if (is_mask) {
-                            const uint64_t bits = (uint64_t)__double_as_longlong(cst[ci + 1]);
+            // small-integer code of the values of columns that IN-set terms
+            // test (64: not an integer in [0, 64))
+            int code[BM_REG_COLS][4];
+            if (ncols <= BM_REG_COLS && mcols) {
 #pragma unroll
-                            for (int j = 0; j < 4; j++) {
-                                const bool in_range = v[j] >= 0.0 && v[j] < 64.0;
-                                const int b = in_range ? (int)v[j] : 0;
-                                ok[j] = ok[j] && in_range && (double)b == v[j] && ((bits >> b) & 1ull);
-                            }
-                            ci += 2;
-                        } else {
-                            const double lo = cst[ci + 1], hi = cst[ci + 2];
-                            const bool lo_open = meta & PV_TERM_LO_OPEN;
-                            const bool hi_open = meta & PV_TERM_HI_OPEN;
-#pragma unroll
-                            for (int j = 0; j < 4; j++) {
-                                const bool a = lo_open ? v[j] > lo : v[j] >= lo;
-                                const bool b = hi_open ? v[j] < hi : v[j] <= hi;
-                                ok[j] = ok[j] && a && b;
-                            }
-                            ci += 3;
-                        }
-                    }
+                for (int cc = 0; cc < BM_REG_COLS; cc++)
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
-                        const uint32_t word = __ballot_sync(0xffffffffu, live[j] && ok[j]);
-                        const uint64_t w = grp * 4 + j;
-                        if (lane == 0 && w < bm_words) {
-                            bitmaps[(uint64_t)(p0 + p) * bm_words + w] = word;
-                            if (word) atomicAdd(&s_cnt[p], (unsigned)__popc(word));
+                        const double x = cv[cc][j];
+                        const bool in = (mcols >> cc) & 1 && x >= 0.0 && x < 64.0;
+                        const int b = in ? (int)x : 64;
+                        code[cc][j] = (in && (double)b == x) ? b : 64;
+                    }
+            }
+            // the 4 words of program p: lanes 0-3 store one each, lane 0
+            // adds their population to the program's count
+            auto store_words = [&](int p, const bool (&b)[4]) {
+                uint32_t wd[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) wd[j] = __ballot_sync(0xffffffffu, b[j]);
+                const uint64_t w = grp * 4 + lane;
+                if (lane < 4 && w < bm_words) {
+                    const uint32_t mine = lane == 0 ? wd[0] : lane == 1 ? wd[1] : lane == 2 ? wd[2] : wd[3];
+                    bitmaps[(uint64_t)(p0 + p) * bm_words + w] = mine;
+                }
+                if (lane == 0) {
+                    const unsigned c = __popc(wd[0]) + __popc(wd[1]) + __popc(wd[2]) + __popc(wd[3]);
+                    if (c) atomicAdd(&s_cnt[p], c);
+                }
+            };
+            for (int p = 0; p < np; p++) {
+                const PredProg pg = s_prog[p];
+                const int nt = s_nt[p];
+                if (nt >= 0) {
+                    // range form: AND of closed intervals and small-integer sets
+                    bool ok[4] = {live[0], live[1], live[2], live[3]};
+                    auto iv = [&](const double (&x)[4], double tlo, double thi) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++) ok[j] = ok[j] && x[j] >= tlo && x[j] <= thi;
+                    };
+                    auto mk = [&](const int (&c)[4], unsigned long long bits) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            ok[j] = ok[j] && c[j] < 64 && ((bits >> (c[j] & 63)) & 1ull);
+                    };
+                    for (int k = 0; k < nt; k++) {
+                        const int tc = s_tcol[p][k];
+                        const int col = tc & 0xFFFF;
+                        const bool is_mask = tc & PV_TERM_MASK;
+                        if (ncols <= BM_REG_COLS) {
+                            if (is_mask) {
+                                const unsigned long long bits = s_tbits[p][k];
+                                switch (col) {
+                                    case 0: mk(code[0], bits); break;
+                                    case 1: mk(code[1], bits); break;
+                                    case 2: mk(code[2], bits); break;
+                                    default: mk(code[3], bits); break;
+                                }
+                            } else {
+                                const double tlo = s_tlo[p][k], thi = s_thi[p][k];
+                                switch (col) {
+                                    case 0: iv(cv[0], tlo, thi); break;
+                                    case 1: iv(cv[1], tlo, thi); break;
+                                    case 2: iv(cv[2], tlo, thi); break;
+                                    default: iv(cv[3], tlo, thi); break;
+                                }
+                            }
+                        } else {
+                            double v[4];
+                            colval(col, v);
+                            if (is_mask) {
+                                int c[4];
+#pragma unroll
+                                for (int j = 0; j < 4; j++) {
+                                    const bool in = v[j] >= 0.0 && v[j] < 64.0;
+                                    const int b = in ? (int)v[j] : 64;
+                                    c[j] = (in && (double)b == v[j]) ? b : 64;
+                                }
+                                mk(c, s_tbits[p][k]);
+                            } else {
+                                iv(v, s_tlo[p][k], s_thi[p][k]);
+                            }
                         }
                     }
+                    store_words(p, ok);
                     continue;
                 }
                 uint64_t st[4] = {0, 0, 0, 0};
@@ -229,15 +311,10 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                         for (int j = 0; j < 4; j++) st[j] ^= 1u;
                     }
                 }
+                bool res[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const uint32_t word = __ballot_sync(0xffffffffu, live[j] && (st[j] & 1u));
-                    const uint64_t w = grp * 4 + j;
-                    if (lane == 0 && w < bm_words) {
-                        bitmaps[(uint64_t)(p0 + p) * bm_words + w] = word;
-                        if (word) atomicAdd(&s_cnt[p], (unsigned)__popc(word));
-                    }
-                }
+                for (int j = 0; j < 4; j++) res[j] = live[j] && (st[j] & 1u);
+                store_words(p, res);
             }
         }
         __syncthreads();

@@ -52,15 +52,15 @@ static_assert(sizeof(PredInsn) == 32, "PredInsn layout");
 
 // Range form of a program (a single instruction of kind PV_NODE_RANGE):
 // the AND of n per-column terms whose encodings sit in the constant pool
-// from val0 on. An interval term is 3 doubles {meta, lo, hi}: lo <= v (or
-// lo < v when open) and v <= hi (v < hi); an IN-set term over small
-// integers is 2 doubles {meta, mask bits}: v is an integer b in [0, 64)
-// with bit b of the mask set. meta = col | kind << 16 | lo_open << 17 |
-// hi_open << 18. Both tests are the f64 comparisons of the nodes they
-// replace (NaN fails every comparison), so results are identical.
+// from val0 on. An interval term is 3 doubles {meta, lo, hi}: lo <= v and
+// v <= hi (open bounds were turned into closed ones on the host); an
+// IN-set term over small integers is 2 doubles {meta, mask bits}: v is an
+// integer b in [0, 64) with bit b of the mask set. meta = col | kind << 16.
+// Both tests are the f64 comparisons of the nodes they replace (NaN fails
+// every comparison), so results are identical.
 constexpr int PV_NODE_RANGE = 16;
 constexpr int PV_RANGE_MAX_TERMS = 4;
-constexpr int PV_TERM_MASK = 1 << 16, PV_TERM_LO_OPEN = 1 << 17, PV_TERM_HI_OPEN = 1 << 18;
+constexpr int PV_TERM_MASK = 1 << 16;
 
 // One distinct predicate of a batch: instructions [insn0, insn0+ninsn).
 struct PredProg {

@@ -217,9 +217,19 @@ bool to_range(const std::vector<PredInsn> &prog, const std::vector<double> &cons
     r.val0 = 0;
     out.assign(1, r);
     outc.clear();
-    for (const Term &t : terms) {
-        const int meta = t.col | (t.mask ? PV_TERM_MASK : 0) | (t.lo_open ? PV_TERM_LO_OPEN : 0) |
-                         (t.hi_open ? PV_TERM_HI_OPEN : 0);
+    for (Term t : terms) {
+        // open bounds become closed ones: on doubles lo < v is lo' <= v with
+        // lo' the next double up (v < hi likewise); an open +inf lower or
+        // -inf upper bound admits nothing (NaN)
+        if (!t.mask && t.lo_open) {
+            t.lo = t.lo == HUGE_VAL ? NAN : nextafter(t.lo, HUGE_VAL);
+            t.lo_open = false;
+        }
+        if (!t.mask && t.hi_open) {
+            t.hi = t.hi == -HUGE_VAL ? NAN : nextafter(t.hi, -HUGE_VAL);
+            t.hi_open = false;
+        }
+        const int meta = t.col | (t.mask ? PV_TERM_MASK : 0);
         outc.push_back((double)meta);
         if (t.mask) {
             double b;

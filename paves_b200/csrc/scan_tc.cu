@@ -758,6 +758,101 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, int stage_
     }
 }
 
+// The same for KO <= 32, without block barriers in the hot loop: each warp
+// keeps its 32 best keys sorted across its lanes (one key per lane) and
+// folds in 32 new keys at a time (a shuffle bitonic sort of the new keys in
+// descending order, an elementwise min with the list, which leaves the 32
+// smallest as a bitonic sequence, and a bitonic clean back to ascending);
+// a batch none of whose keys beats the list's last key is skipped. Warp 0
+// then folds the other warps' lists into its own.
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t x, int lane, bool descending) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint64_t o = __shfl_xor_sync(0xffffffffu, x, j);
+            const bool up = ((lane & k) == 0) != descending;
+            const bool lower = (lane & j) == 0;
+            x = (lower == up) ? (x < o ? x : o) : (x > o ? x : o);
+        }
+    return x;
+}
+
+__device__ __forceinline__ uint64_t warp_clean32(uint64_t x, int lane) {
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const uint64_t o = __shfl_xor_sync(0xffffffffu, x, j);
+        x = (lane & j) == 0 ? (x < o ? x : o) : (x > o ? x : o);
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(DM_THREADS)
+dense_top32_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *__restrict__ dcnt,
+                   int reset_cnt, const unsigned long long *__restrict__ fullmin,
+                   const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
+                   const unsigned long long *__restrict__ popcnt, uint64_t nrows,
+                   FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
+                   uint8_t *__restrict__ trunc, unsigned long long *tau_out,
+                   uint8_t *__restrict__ unc) {
+    constexpr int NW = DM_THREADS / 32;
+    __shared__ uint64_t lists[NW][32];
+    const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned long long bound = tau ? tau[q] : KEY_MAX;
+    uint64_t n = dcnt[q];
+    if (n > dcap) n = dcap;
+    const uint64_t *src = dense + (uint64_t)q * dcap;
+    __syncthreads();
+    if (reset_cnt && tid == 0) dcnt[q] = 0;  // every thread has read it
+    uint64_t best = KEY_MAX;  // ascending across the lanes
+    for (uint64_t b = (uint64_t)warp * 64; b < n; b += NW * 64) {
+        uint64_t k2[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint64_t i = b + u * 32 + lane;
+            k2[u] = i < n ? src[i] : KEY_MAX;
+            if (k2[u] > bound) k2[u] = KEY_MAX;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint64_t worst = __shfl_sync(0xffffffffu, best, 31);
+            if (!__any_sync(0xffffffffu, k2[u] < worst)) continue;
+            const uint64_t d = warp_sort32(k2[u], lane, true);
+            best = warp_clean32(best < d ? best : d, lane);
+        }
+    }
+    lists[warp][lane] = best;
+    __syncthreads();
+    if (warp != 0) return;
+    for (int w = 1; w < NW; w++) {
+        const uint64_t d = lists[w][31 - lane];  // descending
+        const uint64_t m = best < d ? best : d;
+        if (!__any_sync(0xffffffffu, m != best)) continue;
+        best = warp_clean32(m, lane);
+    }
+    const bool have = lane < KO && best != KEY_MAX;
+    const int c = __popc(__ballot_sync(0xffffffffu, have));
+    if (have) {
+        FvHit h;
+        h.node = (uint64_t)key_row(best);
+        h.dist = key_dist(best);
+        out[(uint64_t)q * KO + lane] = h;
+    }
+    const uint64_t last = __shfl_sync(0xffffffffu, best, KO - 1);
+    if (lane == 0) {
+        out_cnt[q] = (uint32_t)c;
+        const int pg = qprog[q];
+        const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
+        trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
+        if (tau_out && c == KO && last < tau_out[q]) tau_out[q] = last;
+        if (unc) {
+            const unsigned long long lim = c == KO ? last : bound;
+            const unsigned long long fm = fullmin ? fullmin[q] : KEY_MAX;
+            unc[q] = (fm != KEY_MAX && fm <= lim) ? 1 : 0;
+        }
+    }
+}
+
 cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,
                                bool reset_cnt, const unsigned long long *fullmin,
                                const unsigned long long *tau, int KO, const int32_t *qprog,
@@ -765,6 +860,12 @@ cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *d
                                FvHit *out, uint32_t *out_cnt, uint8_t *trunc,
                                unsigned long long *tau_out, uint8_t *unc, cudaStream_t st) {
     if (KO < 1 || KO > DM_OUT) return cudaErrorInvalidValue;
+    if (KO <= 32) {
+        dense_top32_kernel<<<nq, DM_THREADS, 0, st>>>(dense, dcap, dcnt, reset_cnt ? 1 : 0,
+                                                      fullmin, tau, KO, qprog, popcnt, nrows, out,
+                                                      out_cnt, trunc, tau_out, unc);
+        return cudaGetLastError();
+    }
     // the stage holds a whole run when it can (runs never exceed dcap)
     const int stage_cap = (int)std::min<uint64_t>(std::max<uint64_t>(dcap, 1), DM_CAP_MAX);
     const size_t smem = (size_t)(stage_cap + DM_OUT) * 8;

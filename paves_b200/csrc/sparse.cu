@@ -103,13 +103,9 @@ uint64_t prog_upper_bound(const FvGpuIndex *g, const PredInsn *ins, int n, const
                         ci += 2;
                     } else {
                         const double lo = consts[ci + 1], hi_v = consts[ci + 2];
-                        if (lo == lo && hi_v == hi_v) {
-                            const uint64_t a = (meta & PV_TERM_LO_OPEN)
-                                                   ? std::upper_bound(v.begin(), v.end(), lo) - v.begin()
-                                                   : std::lower_bound(v.begin(), v.end(), lo) - v.begin();
-                            const uint64_t b = (meta & PV_TERM_HI_OPEN)
-                                                   ? std::lower_bound(v.begin(), v.end(), hi_v) - v.begin()
-                                                   : std::upper_bound(v.begin(), v.end(), hi_v) - v.begin();
+                        if (lo == lo && hi_v == hi_v) {  // closed [lo, hi]
+                            const uint64_t a = std::lower_bound(v.begin(), v.end(), lo) - v.begin();
+                            const uint64_t b = std::upper_bound(v.begin(), v.end(), hi_v) - v.begin();
                             c = b > a ? b - a : 0;
                         }
                         ci += 3;
