@@ -237,7 +237,7 @@ KERNEL_CASES = {
 def kernel_case(name, iters, tc_shape=None):
     """One batch shape run `iters` times after 3 warm-up runs (device-
     resident inputs): the small, self-contained program that ncu captures
-    profile. tc_shape = (epi, stages, grow, replicas), 0 = automatic."""
+    profile. tc_shape = (epi, stages, grow, replicas, seed), 0 = automatic."""
     nq, prec, mode, pk = KERNEL_CASES[name]
     if name == "graph_b64":
         from paves_b200.hnsw import Hnsw
@@ -460,7 +460,8 @@ def main():
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES),
                     help="run one batch shape --steps times and exit (for profilers)")
     ap.add_argument("--tc-shape", default=None,
-                    help="kernel cases: tensor-core shape epi,stages,grow,replicas (0 = auto)")
+                    help="kernel cases: tensor-core shape epi,stages,grow,replicas,seed "
+                         "(0 = auto; seed 2 = no seeding pass)")
     args = ap.parse_args()
     if args.workload == "stream":
         stream_bench(args)
@@ -469,7 +470,10 @@ def main():
         graph_bench(args)
         return
     if args.kernel_case:
-        shape = tuple(int(x) for x in args.tc_shape.split(",")) if args.tc_shape else None
+        shape = None
+        if args.tc_shape:
+            shape = tuple(int(x) for x in args.tc_shape.split(","))
+            shape = shape + (0,) * (5 - len(shape))
         kernel_case(args.kernel_case, max(1, args.steps), shape)
         return
     args.warmup = max(3, args.warmup)

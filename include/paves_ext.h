@@ -317,8 +317,10 @@ int pv_last_sparse(const FvGpuIndex *g);
 /* Shape of the tensor-core scan for later batches on g (0 = automatic):
  * epilogue warp groups (1, 2), pipeline stages (2..8), CTAs along rows per
  * query tile, query replicas down the tile (1, 2, 4; capped so that each
- * replica's share of a 128-row tile is at least 32 rows). -1: bad value. */
-int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep);
+ * replica's share of a 128-row tile is at least 32 rows), seeding pass
+ * (1 = always when the index has 8+ tiles per CTA, 2 = never; the main
+ * pass then bounds itself from its own lists). -1: bad value. */
+int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, int seed);
 int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,
                     uint64_t *bound, char *errbuf, size_t errlen);

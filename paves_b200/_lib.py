@@ -194,6 +194,6 @@ _EXT_SIGS.update({
     "pv_stream_free": (None, [P]),
 })
 _EXT_SIGS["pv_last_sparse"] = (C.c_int, [P])
-_EXT_SIGS["pv_tc_shape"] = (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int])
+_EXT_SIGS["pv_tc_shape"] = (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int])
 _EXT_SIGS["pv_filter_bound"] = (C.c_int, [P, P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_char_p,
                                           C.c_size_t])

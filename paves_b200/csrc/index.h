@@ -115,7 +115,7 @@ struct FvGpuIndex {
     int last_uncertain = 0;  // queries of the last call re-run exactly (or flagged)
     // tensor-core scan shape overrides (0 = built-in choice): epilogue warp
     // groups, pipeline stages, CTAs along the rows per query tile
-    int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0;
+    int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0, tune_seed = 0;
     bool view = false;  // shares another handle's device data, owns only scratch
     int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels

@@ -300,14 +300,19 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             }
             g = qvalid ? *((volatile unsigned long long *)(a.tau + qg)) : KEY_MAX;
         };
+        // two tiles ahead: a tile's epilogue is shorter than a load's latency
+        float nxr[CPH], nxs[CPH];
+        uint32_t nbw[CPH];
+        unsigned long long ngt = KEY_MAX;
         if (ntiles) load_tile(0, xr, xs, bw, gt);
+        if (ntiles > 1) load_tile(1, nxr, nxs, nbw, ngt);
         for (uint64_t t = 0; t < ntiles; t++) {
             const int acc = (int)(t & 1);
             const uint32_t aph = (uint32_t)((t >> 1) & 1);
-            float nxr[CPH], nxs[CPH];
-            uint32_t nbw[CPH];
-            unsigned long long ngt = KEY_MAX;
-            if (t + 1 < ntiles) load_tile(t + 1, nxr, nxs, nbw, ngt);
+            float n2xr[CPH], n2xs[CPH];
+            uint32_t n2bw[CPH];
+            unsigned long long n2gt = KEY_MAX;
+            if (t + 2 < ntiles) load_tile(t + 2, n2xr, n2xs, n2bw, n2gt);
             if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) { ok = false; break; }
             tc_fence_after();
             const bool tr = a.trace && blockIdx.x == 0 && slot == 0 && t < (uint64_t)a.trace_tiles;
@@ -399,8 +404,12 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 xr[j] = nxr[j];
                 xs[j] = nxs[j];
                 bw[j] = nbw[j];
+                nxr[j] = n2xr[j];
+                nxs[j] = n2xs[j];
+                nbw[j] = n2bw[j];
             }
             gt = ngt;
+            ngt = n2gt;
         }
         if (!ok) {
             s_abort = 1;
@@ -1101,7 +1110,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     // Seeding pass: a few tiles per CTA from an evenly strided sample; the
     // merged K'-th key of the sample bounds the K'-th key of the whole
     // scan, so the main pass admits only rows that can still matter.
-    if (ntiles_all >= 8 * (uint64_t)grow) {
+    const bool seed = g->tune_seed == 2 ? false : ntiles_all >= 8 * (uint64_t)grow;
+    if (seed) {
         TcArgs sa = a;
         // larger supersets take a larger sample (up to 8 tiles per CTA,
         // spread over the CTA's own range), so the bound stays near the
@@ -1113,9 +1123,16 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sa.tile_step = std::max<uint64_t>(1, region / m);
         sa.tiles_per_cta = m;
         // only each list's best keys: the S-th key of a subset of the
-        // sample still bounds the S-th key of the scan, and the subset
-        // stays within the merge's shared-memory stage
-        sa.kwrite = std::max(1, std::min(KP, DM_CAP_MAX / std::max(1, nlists)));
+        // sample still bounds the S-th key of the scan, and a short run
+        // keeps the merge cheap (the radix select of S > 32 reads its run
+        // 8 times; the S-th best of the sample rarely needs more than a
+        // few keys of any one list)
+        const int seed_keys = S <= 32 ? 8192 : 4096;
+        sa.kwrite = std::max(1, std::min(KP, seed_keys / std::max(1, nlists)));
+        // lists need hold no more than that (short heaps admit fewer rows);
+        // a full list's last key bounds the S-th key only if it holds S
+        sa.KP = sa.kwrite;
+        sa.push_tau = sa.KP == S ? 1 : 0;
         sa.fullmin = nullptr;
         g->launches += 2;  // seeding pass + its merge
         PV_CUDA_OK(run(sa), errbuf, errlen);

@@ -147,7 +147,7 @@ def test_tc_epilogue_shapes_match_oracle(epi, rep, nq):
     L = _lib.lib()
     ds = datagen.make_dataset(90_001, 128, nq=nq)
     gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_BF16)
-    assert L.pv_tc_shape(gi.handle, epi, 0, 0, rep) == 0
+    assert L.pv_tc_shape(gi.handle, epi, 0, 0, rep, 2 if rep == 2 else 0) == 0
     six = list(datagen.six_predicates().values()) + [None]
     preds = [six[(q + 3) % len(six)] for q in range(nq)]
     bp = pred.concat(preds, len(ds.vectors))
@@ -161,5 +161,5 @@ def test_tc_epilogue_shapes_match_oracle(epi, rep, nq):
             assert np.array_equal(ids[q, :n], o_ids[q, :n].astype(np.uint64)), (q, topb)
             assert np.array_equal(dists[q, :n], o_d32[q, :n]), (q, topb)
             assert trunc[q] == (o_pass[q] > topb)
-    assert L.pv_tc_shape(gi.handle, 0, 0, 0, 3) == -1
+    assert L.pv_tc_shape(gi.handle, 0, 0, 0, 3, 0) == -1
     gi.close()
