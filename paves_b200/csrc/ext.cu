@@ -68,7 +68,9 @@ extern "C" PvBatch *pv_batch_create(FvGpuIndex *g, int nq, const float *queries,
         pv_batch_free(b);
         return nullptr;
     }
-    cudaError_t e = cudaMemcpy(b->stage_d.p, b->stage_h.p, b->db.bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(b->stage_d.p, b->stage_h.p, b->db.bytes,
+                                    cudaMemcpyHostToDevice, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
     if (e != cudaSuccess) return fail("upload", e);
     const size_t hit = (size_t)nq * topb * sizeof(FvHit);
     b->off_cnt = (hit + 255) & ~(size_t)255;
@@ -131,8 +133,11 @@ extern "C" int pv_batch_fetch(PvBatch *b, FvHit *out, uint32_t *out_cnt, uint8_t
     FvGpuIndex *g = b->g;
     std::lock_guard<std::mutex> lk(g->mu);
     PV_CUDA_OK(cudaSetDevice(g->device), errbuf, errlen);
-    PV_CUDA_OK(cudaMemcpy(b->out_h.p, b->out_d.p, b->obytes, cudaMemcpyDeviceToHost), errbuf,
-               errlen);
+    // in the order of the batch's own stream
+    PV_CUDA_OK(cudaMemcpyAsync(b->out_h.p, b->out_d.p, b->obytes, cudaMemcpyDeviceToHost,
+                               g->stream),
+               errbuf, errlen);
+    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
     const int nq = b->db.nq;
     const char *oh = b->out_h.as<char>();
     const uint32_t *cnt = (const uint32_t *)(oh + b->off_cnt);
@@ -147,8 +152,10 @@ extern "C" int pv_batch_fetch(PvBatch *b, FvHit *out, uint32_t *out_cnt, uint8_t
     g->last_uncertain = 0;
     if (g->tc_unc && g->tc_unc_n == nq) {
         std::vector<uint8_t> unc((size_t)nq);
-        PV_CUDA_OK(cudaMemcpy(unc.data(), g->tc_unc, (size_t)nq, cudaMemcpyDeviceToHost), errbuf,
-                   errlen);
+        PV_CUDA_OK(cudaMemcpyAsync(unc.data(), g->tc_unc, (size_t)nq, cudaMemcpyDeviceToHost,
+                                   g->stream),
+                   errbuf, errlen);
+        PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
         for (int q = 0; q < nq; q++) g->last_uncertain += unc[q] ? 1 : 0;
     }
     return 0;

@@ -265,27 +265,31 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
     cudaEventCreate(&g->ev0);
     cudaEventCreate(&g->ev1);
 
+    // every copy and fill of the upload runs on g->stream, in order with the
+    // conversion kernels (the library's streams do not wait for the legacy
+    // default stream, and a fill of device memory returns before it runs)
     if ((e = cudaMalloc(&g->d_vecs, count * (size_t)dpad * 4)) != cudaSuccess)
         return bail("rows", e);
     if (dpad == dim) {
-        e = cudaMemcpy(g->d_vecs, vectors, count * (size_t)dim * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(g->d_vecs, vectors, count * (size_t)dim * 4, cudaMemcpyHostToDevice,
+                            g->stream);
     } else {
-        if ((e = cudaMemset(g->d_vecs, 0, count * (size_t)dpad * 4)) == cudaSuccess)
-            e = cudaMemcpy2D(g->d_vecs, (size_t)dpad * 4, vectors, (size_t)dim * 4,
-                             (size_t)dim * 4, count, cudaMemcpyHostToDevice);
+        if ((e = cudaMemsetAsync(g->d_vecs, 0, count * (size_t)dpad * 4, g->stream)) == cudaSuccess)
+            e = cudaMemcpy2DAsync(g->d_vecs, (size_t)dpad * 4, vectors, (size_t)dim * 4,
+                                  (size_t)dim * 4, count, cudaMemcpyHostToDevice, g->stream);
     }
     if (e != cudaSuccess) return bail("rows copy", e);
 
     if (ncols > 0) {
         if ((e = cudaMalloc(&g->d_cols, count * (size_t)ncols * 8)) != cudaSuccess)
             return bail("columns", e);
-        if ((e = cudaMemcpy(g->d_cols, cols, count * (size_t)ncols * 8,
-                            cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(g->d_cols, cols, count * (size_t)ncols * 8,
+                                 cudaMemcpyHostToDevice, g->stream)) != cudaSuccess)
             return bail("columns copy", e);
         if ((e = cudaMalloc(&g->d_prows, count * (size_t)ncols * 4)) != cudaSuccess)
             return bail("postings", e);
-        if ((e = cudaMemcpy(g->d_prows, post_rows, count * (size_t)ncols * 4,
-                            cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(g->d_prows, post_rows, count * (size_t)ncols * 4,
+                                 cudaMemcpyHostToDevice, g->stream)) != cudaSuccess)
             return bail("postings copy", e);
         pv::build_sorted_cols(g, cols, post_rows);
     }
@@ -295,7 +299,8 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         uint32_t *d_l0 = nullptr;
         if ((e = cudaMalloc(&d_l0, count * (size_t)l0_stride * 4)) != cudaSuccess)
             return bail("graph staging", e);
-        e = cudaMemcpy(d_l0, l0, count * (size_t)l0_stride * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(d_l0, l0, count * (size_t)l0_stride * 4, cudaMemcpyHostToDevice,
+                            g->stream);
         if (e == cudaSuccess) e = cudaMalloc(&g->d_adj, count * (size_t)g->deg_cap * 4);
         if (e == cudaSuccess) e = cudaMalloc(&g->d_deg, count * 2);
         if (e == cudaSuccess) {
@@ -316,12 +321,13 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         if ((e = cudaMalloc(&g->d_vlow, count * (size_t)kpad * esz)) != cudaSuccess)
             return bail("low-precision rows", e);
         if ((e = cudaMalloc(&g->d_norm, rows_pad * 4)) != cudaSuccess) return bail("norms", e);
-        if ((e = cudaMemset(g->d_norm, 0, rows_pad * 4)) != cudaSuccess) return bail("norms", e);
+        if ((e = cudaMemsetAsync(g->d_norm, 0, rows_pad * 4, g->stream)) != cudaSuccess)
+            return bail("norms", e);
         unsigned blocks = (unsigned)((count + 7) / 8);
         if (f8) {
             if ((e = cudaMalloc(&g->d_vscale, rows_pad * 4)) != cudaSuccess)
                 return bail("scales", e);
-            if ((e = cudaMemset(g->d_vscale, 0, rows_pad * 4)) != cudaSuccess)
+            if ((e = cudaMemsetAsync(g->d_vscale, 0, rows_pad * 4, g->stream)) != cudaSuccess)
                 return bail("scales", e);
             to_fp8_kernel<<<blocks, 256, 0, g->stream>>>(g->d_vecs, dpad, dim, count,
                                                          (__nv_fp8_e4m3 *)g->d_vlow, kpad,
@@ -332,8 +338,9 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
                                                           g->d_norm);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return bail("convert", e);
-        if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail("convert", e);
     }
+    // the caller's arrays may go once this returns
+    if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail("upload", e);
     return g;
 }
 

@@ -116,6 +116,14 @@ struct FvGpuIndex {
     // tensor-core scan shape overrides (0 = built-in choice): epilogue warp
     // groups, pipeline stages, CTAs along the rows per query tile
     int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0, tune_seed = 0;
+    // encoded TMA descriptors of the tensor-core scan (CUtensorMap, 128 B):
+    // the rows' (fixed after upload) and the staged queries' (re-encoded
+    // when their buffer or row count changes)
+    alignas(64) unsigned char tmap_x[128] = {};
+    alignas(64) unsigned char tmap_q[128] = {};
+    bool tmap_x_ok = false;
+    const void *tmap_q_ptr = nullptr;
+    uint64_t tmap_q_rows = 0;
     bool view = false;  // shares another handle's device data, owns only scratch
     int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels

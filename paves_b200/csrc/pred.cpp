@@ -243,6 +243,87 @@ bool to_range(const std::vector<PredInsn> &prog, const std::vector<double> &cons
     return true;
 }
 
+// Structural hash and equality of node trees, straight from the ABI arrays
+// (no allocation): identical predicates in different slices of the
+// concatenated arrays are found before any program is built. hash returns
+// false on anything the walker would reject; such queries take the walker,
+// which reports the error.
+struct TreeView {
+    const FvGpuPredNode *nodes;
+    int nnodes;
+    const int32_t *children;
+    int nchildren;
+    const double *invals;
+    int ninvals;
+
+    static uint64_t mix(uint64_t h, uint64_t v) {
+        h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+        return h;
+    }
+    static uint64_t bits(double v) {
+        uint64_t b;
+        memcpy(&b, &v, 8);
+        return b;
+    }
+    bool child_range(const FvGpuPredNode &n) const {
+        return n.nchildren >= 0 && n.child0 >= 0 && (int64_t)n.child0 + n.nchildren <= nchildren;
+    }
+    bool hash(int ni, int level, int &budget, uint64_t &h) const {
+        if (ni < 0 || ni >= nnodes || --budget < 0 || level > 60) return false;
+        const FvGpuPredNode &n = nodes[ni];
+        h = mix(h, (uint64_t)(uint32_t)n.kind);
+        switch (n.kind) {
+            case FV_NODE_CMP:
+                h = mix(mix(mix(h, (uint64_t)(uint32_t)n.col), (uint64_t)(uint32_t)n.op), bits(n.value));
+                return true;
+            case FV_NODE_IN:
+                if (n.nvalues < 0 || n.val0 < 0 || (int64_t)n.val0 + n.nvalues > ninvals) return false;
+                h = mix(mix(h, (uint64_t)(uint32_t)n.col), (uint64_t)(uint32_t)n.nvalues);
+                for (int i = 0; i < n.nvalues; i++) h = mix(h, bits(invals[n.val0 + i]));
+                return true;
+            case FV_NODE_AND:
+            case FV_NODE_OR:
+            case FV_NODE_NOT: {
+                const int nc = n.kind == FV_NODE_NOT ? 1 : n.nchildren;
+                if (n.kind == FV_NODE_NOT ? (n.nchildren < 1 || n.child0 < 0 || n.child0 >= nchildren)
+                                          : !child_range(n))
+                    return false;
+                h = mix(h, (uint64_t)(uint32_t)nc);
+                for (int i = 0; i < nc; i++)
+                    if (!hash(children[n.child0 + i], level + 1, budget, h)) return false;
+                return true;
+            }
+            default:
+                return false;
+        }
+    }
+    // a and b were both hashed successfully
+    bool equal(int a, int b, int level) const {
+        if (a == b) return true;
+        if (level > 60) return false;
+        const FvGpuPredNode &x = nodes[a], &y = nodes[b];
+        if (x.kind != y.kind) return false;
+        switch (x.kind) {
+            case FV_NODE_CMP:
+                return x.col == y.col && x.op == y.op && bits(x.value) == bits(y.value);
+            case FV_NODE_IN:
+                if (x.col != y.col || x.nvalues != y.nvalues) return false;
+                for (int i = 0; i < x.nvalues; i++)
+                    if (bits(invals[x.val0 + i]) != bits(invals[y.val0 + i])) return false;
+                return true;
+            default: {
+                const int nx = x.kind == FV_NODE_NOT ? 1 : x.nchildren;
+                const int ny = y.kind == FV_NODE_NOT ? 1 : y.nchildren;
+                if (nx != ny) return false;
+                for (int i = 0; i < nx; i++)
+                    if (!equal(children[x.child0 + i], children[y.child0 + i], level + 1))
+                        return false;
+                return true;
+            }
+        }
+    }
+};
+
 }  // namespace
 
 // Compiles the per-query predicates of a batch. Returns 0, or -1 + errbuf.
@@ -261,8 +342,18 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
         return -1;
     }
     std::unordered_map<std::string, int> seen;
-    // identical roots map to the same program without re-walking
-    std::unordered_map<int32_t, int> by_root;
+    // structurally identical trees (the same root included) share one
+    // program without re-walking: an open-addressing table of
+    // (hash, representative root, program)
+    const TreeView tv{nodes, nnodes, children, nchildren, invals, ninvals};
+    struct Rep {
+        uint64_t h;
+        int32_t root;
+        int pid;
+    };
+    size_t tsize = 16;
+    while (tsize < 2 * (size_t)nq) tsize <<= 1;
+    std::vector<Rep> reps(tsize, Rep{0, -1, -1});
     for (int q = 0; q < nq; q++) {
         int32_t root = *(const int32_t *)((const char *)proot + (size_t)q * proot_stride);
         if (root < 0) continue;
@@ -271,10 +362,21 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
                      q, root, nnodes);
             return -1;
         }
-        auto br = by_root.find(root);
-        if (br != by_root.end()) {
-            pb.qprog[q] = br->second;
-            continue;
+        uint64_t h = 0;
+        int hb = 4 * nnodes + 16;
+        const bool hashed = tv.hash(root, 0, hb, h);
+        size_t slot = (size_t)(h ^ (h >> 29)) & (tsize - 1);
+        if (hashed) {
+            int hit = -1;
+            for (; reps[slot].root >= 0; slot = (slot + 1) & (tsize - 1))
+                if (reps[slot].h == h && tv.equal(reps[slot].root, root, 0)) {
+                    hit = reps[slot].pid;
+                    break;
+                }
+            if (hit >= 0) {
+                pb.qprog[q] = hit;
+                continue;
+            }
         }
         Walker w{nodes, nnodes, children, nchildren, invals, ninvals, ncols, {}, {}, 4 * nnodes + 16};
         if (!w.emit(root, 0)) {
@@ -331,7 +433,7 @@ int compile_predicates(int nq, const int32_t *proot, size_t proot_stride,
             pb.cols_used.push_back(colmask);
             seen.emplace(std::move(sig), pid);
         }
-        by_root.emplace(root, pid);
+        if (hashed) reps[slot] = Rep{h, root, pid};  // the free slot the probe stopped at
         pb.qprog[q] = pid;
     }
     return 0;

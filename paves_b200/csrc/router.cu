@@ -446,12 +446,16 @@ extern "C" PvRouter *pv_router_create(int device, const float *centroids, int nc
     for (int c = 0; c < ncent; c++)
         memcpy(&pad[(size_t)c * r->dpad], centroids + (size_t)c * dim, sizeof(float) * dim);
     if ((e = cudaMalloc(&r->d_cent, pad.size() * 4)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpy(r->d_cent, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+    // on r->stream, in order with the router's kernels (a non-blocking
+    // stream does not wait for the legacy default stream)
+    if ((e = cudaMemcpyAsync(r->d_cent, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice,
+                             r->stream)) != cudaSuccess)
         return fail(e);
     char *blk = nullptr;
     const size_t bytes = (size_t)P_N * (4 * 4 + 2) + 2 * NI * 4 + 256 * 6;
     if ((e = cudaMalloc(&blk, bytes)) != cudaSuccess) return fail(e);
-    cudaMemset(blk, 0, bytes);
+    if ((e = cudaMemsetAsync(blk, 0, bytes, r->stream)) != cudaSuccess) return fail(e);
+    if ((e = cudaStreamSynchronize(r->stream)) != cudaSuccess) return fail(e);
     size_t o = 0;
     auto carve = [&](size_t n) { char *p = blk + o; o += (n + 255) & ~(size_t)255; return p; };
     r->mlp.master = (float *)carve((size_t)P_N * 4);
@@ -504,9 +508,13 @@ extern "C" int pv_router_get_params(PvRouter *r, float *params, float *feat_mean
     std::lock_guard<std::mutex> lk(r->mu);
     if (cudaSetDevice(r->device) != cudaSuccess) return -1;
     float norm[2 * NI];
-    if (params && cudaMemcpy(params, r->mlp.master, (size_t)P_N * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (params && cudaMemcpyAsync(params, r->mlp.master, (size_t)P_N * 4,
+                                  cudaMemcpyDeviceToHost, r->stream) != cudaSuccess)
         return -1;
-    if (cudaMemcpy(norm, r->mlp.norm, sizeof(norm), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(norm, r->mlp.norm, sizeof(norm), cudaMemcpyDeviceToHost, r->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(r->stream) != cudaSuccess)
+        return -1;
     if (feat_mean) memcpy(feat_mean, norm, NI * 4);
     if (feat_std) memcpy(feat_std, norm + NI, NI * 4);
     return 0;
@@ -785,7 +793,9 @@ extern "C" int pv_router_train(PvRouter *r, int n, const float *feats, const int
     if (graph) cudaGraphDestroy(graph);
     RT_OK(err);
     std::vector<float> lh(epochs);
-    RT_OK(cudaMemcpy(lh.data(), t.loss, (size_t)epochs * 4, cudaMemcpyDeviceToHost));
+    RT_OK(cudaMemcpyAsync(lh.data(), t.loss, (size_t)epochs * 4, cudaMemcpyDeviceToHost,
+                          r->stream));
+    RT_OK(cudaStreamSynchronize(r->stream));
     // each step added its batch mean: report the epoch mean
     if (epoch_loss)
         for (int e = 0; e < epochs; e++) epoch_loss[e] = lh[e] / (float)spe;

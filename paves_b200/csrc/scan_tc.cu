@@ -1056,12 +1056,28 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         certify ? d_fullmin : nullptr, d_err);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
 
+    static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
-    if (!make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count) ||
-        !make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
-        snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
-        return -1;
+    if (!g->tmap_x_ok) {
+        if (!make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count)) {
+            snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
+            return -1;
+        }
+        memcpy(g->tmap_x, &tmX, sizeof(tmX));
+        g->tmap_x_ok = true;
     }
+    memcpy(&tmX, g->tmap_x, sizeof(tmX));
+    if (g->tmap_q_ptr != c || g->tmap_q_rows != (uint64_t)nqpad) {
+        if (!make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
+            g->tmap_q_ptr = nullptr;
+            snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
+            return -1;
+        }
+        memcpy(g->tmap_q, &tmQ, sizeof(tmQ));
+        g->tmap_q_ptr = c;
+        g->tmap_q_rows = (uint64_t)nqpad;
+    }
+    memcpy(&tmQ, g->tmap_q, sizeof(tmQ));
     TcArgs a;
     a.nrows = g->count;
     a.kblocks = kblocks;
@@ -1180,9 +1196,11 @@ namespace pv {
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen) {
     if (!g->tc_err) return 0;
     int e = 0;
-    PV_CUDA_OK(cudaMemcpy(&e, g->tc_err, 4, cudaMemcpyDeviceToHost), errbuf, errlen);
+    PV_CUDA_OK(cudaMemcpyAsync(&e, g->tc_err, 4, cudaMemcpyDeviceToHost, g->stream), errbuf,
+               errlen);
+    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
     if (e) {
-        cudaMemset(g->tc_err, 0, 4);
+        cudaMemsetAsync(g->tc_err, 0, 4, g->stream);
         snprintf(errbuf, errlen, "gpu: tensor-core scan wait expired (role %d)", e);
         return -1;
     }

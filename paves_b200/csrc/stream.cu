@@ -433,8 +433,10 @@ extern "C" int pv_stream_run(PvStream *s, int nq, const float *queries, const Fv
     }
     if (b->d_unc) {
         std::vector<uint8_t> unc(b->B);
-        PV_CUDA_OK(cudaMemcpy(unc.data(), b->d_unc, (size_t)b->B, cudaMemcpyDeviceToHost), errbuf,
-                   errlen);
+        PV_CUDA_OK(cudaMemcpyAsync(unc.data(), b->d_unc, (size_t)b->B, cudaMemcpyDeviceToHost,
+                                   v->stream),
+                   errbuf, errlen);
+        PV_CUDA_OK(cudaStreamSynchronize(v->stream), errbuf, errlen);
         int n = 0;
         for (int q = 0; q < nq; q++) n += unc[q] ? 1 : 0;
         if (n) {
