@@ -163,3 +163,21 @@ def test_tc_epilogue_shapes_match_oracle(epi, rep, nq):
             assert trunc[q] == (o_pass[q] > topb)
     assert L.pv_tc_shape(gi.handle, 0, 0, 0, 3, 0) == -1
     gi.close()
+
+
+def test_fresh_fp8_indexes_convert_every_row():
+    """Uploads order their copies, fills and the FP8 conversion on one
+    stream: a fill left on the default stream once raced the conversion
+    and zeroed row scales of about one FP8 index in a hundred (rows then
+    looked far from every query). Many fresh small indexes, one batch
+    each, all at the recall bar."""
+    n, d = 5000, 96
+    ds = datagen.make_dataset(n, d, nq=32, ncomp=64)
+    bp = pred.concat([None, datagen.six_predicates()["sel70%"]] * 16, n)
+    o_ids, _, _, o_cnt, _ = cpu.exact_topk(ds.vectors, ds.cols, ds.queries, bp, 10)
+    for i in range(200):
+        gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_FP8)
+        ids, _, _, _ = gi.brute_batch_raw(ds.queries, bp, 10)
+        gi.close()
+        r = recall(ids.astype(np.int64), o_ids.astype(np.int64), o_cnt, 10)
+        assert r >= 0.95, (i, r)
