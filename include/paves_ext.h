@@ -314,6 +314,27 @@ int pv_last_uncertain(const FvGpuIndex *g);
  * took this route. pv_filter_bound: the bound for one filter (node 0 is
  * the root; nnodes 0 = no filter -> count). */
 int pv_last_sparse(const FvGpuIndex *g);
+/* Stored device layout. No reference counterpart: the reference converts
+ * its rows at every upload (gpu_engine.cu:1692-1773). The low-precision
+ * rows ([count][kpad], kpad = dim rounded up to 64 for BF16 / 128 for FP8),
+ * their norms and FP8 scales (f32 [count]) are read back with
+ * pv_index_export (PV_PART_*; pv_index_part_bytes gives each part's size,
+ * -1 if the index has no such part) and stored beside the index file; a
+ * later pv_index_upload_prepared copies them back instead of converting,
+ * and takes the stored row_amax (the BF16 exactness certificate's input)
+ * instead of scanning every row on the host. Arguments otherwise as
+ * fv_gpu_index_upload; NULL on error with the message in errbuf. */
+enum { PV_PART_LOWP_ROWS = 1, PV_PART_NORMS = 2, PV_PART_SCALES = 3 };
+int64_t pv_index_part_bytes(const FvGpuIndex *g, int part);
+int pv_index_export(FvGpuIndex *g, int part, void *dst, uint64_t bytes, float *row_amax,
+                    char *errbuf, size_t errlen);
+FvGpuIndex *pv_index_upload_prepared(const float *vectors, const double *cols,
+                                     const uint32_t *post_rows, const uint32_t *l0,
+                                     uint32_t l0_stride, uint64_t count, int dim, int ncols,
+                                     int device, int precision, const void *vlow,
+                                     const float *norms, const float *scales, float row_amax,
+                                     char *errbuf, size_t errlen);
+
 /* Shape of the tensor-core scan for later batches on g (0 = automatic):
  * epilogue warp groups (1, 2), pipeline stages (2..8), CTAs along rows per
  * query tile, query replicas down the tile (1, 2, 4; capped so that each

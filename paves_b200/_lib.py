@@ -194,6 +194,12 @@ _EXT_SIGS.update({
     "pv_stream_free": (None, [P]),
 })
 _EXT_SIGS["pv_last_sparse"] = (C.c_int, [P])
+_EXT_SIGS["pv_index_part_bytes"] = (C.c_int64, [P, C.c_int])
+_EXT_SIGS["pv_index_export"] = (C.c_int, [P, C.c_int, P, C.c_uint64, P, C.c_char_p, C.c_size_t])
+_EXT_SIGS["pv_index_upload_prepared"] = (P, [P, P, P, P, C.c_uint32, C.c_uint64, C.c_int, C.c_int,
+                                             C.c_int, C.c_int, P, P, P, C.c_float, C.c_char_p,
+                                             C.c_size_t])
+PV_PART_LOWP_ROWS, PV_PART_NORMS, PV_PART_SCALES = 1, 2, 3
 _EXT_SIGS["pv_tc_shape"] = (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int])
 _EXT_SIGS["pv_filter_bound"] = (C.c_int, [P, P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_char_p,
                                           C.c_size_t])

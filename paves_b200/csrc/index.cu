@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "index.h"
+#include "paves_ext.h"
 #include "pv_internal.h"
 
 namespace pv {
@@ -212,11 +213,21 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
     delete g;
 }
 
-extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *cols,
-                                           const uint32_t *post_rows, const uint32_t *l0,
-                                           uint32_t l0_stride, uint64_t count, int dim,
-                                           int ncols, int device, int precision,
-                                           char *errbuf, size_t errlen) {
+namespace {
+
+// Low-precision rows, norms and scales made by an earlier upload (read back
+// with pv_index_export and stored beside the index file).
+struct Prepared {
+    const void *vlow;
+    const float *norm;
+    const float *scale;  // FP8 only
+    float row_amax;
+};
+
+FvGpuIndex *upload_impl(const float *vectors, const double *cols, const uint32_t *post_rows,
+                        const uint32_t *l0, uint32_t l0_stride, uint64_t count, int dim,
+                        int ncols, int device, int precision, const Prepared *prep,
+                        char *errbuf, size_t errlen) {
     auto fail = [&](const char *what, cudaError_t e) -> FvGpuIndex * {
         if (errbuf && errlen)
             snprintf(errbuf, errlen, "gpu: index upload: %s%s%s", what, e ? ": " : "",
@@ -230,6 +241,9 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
     if (precision < FV_GPU_PREC_FP32 || precision > FV_GPU_PREC_FP8)
         return fail("unknown precision", cudaSuccess);
     if (l0 && l0_stride < 2) return fail("bad l0 stride", cudaSuccess);
+    if (prep && (precision == FV_GPU_PREC_FP32 || !prep->vlow || !prep->norm ||
+                 (precision == FV_GPU_PREC_FP8 && !prep->scale)))
+        return fail("prepared arrays missing for this precision", cudaSuccess);
 
     const int dpad = (dim + 3) & ~3;
     // low-precision row stride: whole 128-byte swizzle rows
@@ -313,7 +327,8 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         if (e != cudaSuccess) return bail("graph", e);
     }
 
-    g->row_amax = pv_integral_amax(vectors, count * (uint64_t)dim);
+    // the BF16 exactness certificate's input: scanned here, or stored
+    g->row_amax = prep ? prep->row_amax : pv_integral_amax(vectors, count * (uint64_t)dim);
 
     if (precision != FV_GPU_PREC_FP32) {
         const bool f8 = precision == FV_GPU_PREC_FP8;
@@ -324,7 +339,21 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
         if ((e = cudaMemsetAsync(g->d_norm, 0, rows_pad * 4, g->stream)) != cudaSuccess)
             return bail("norms", e);
         unsigned blocks = (unsigned)((count + 7) / 8);
-        if (f8) {
+        if (prep) {
+            // straight copies of the stored device layout
+            e = cudaMemcpyAsync(g->d_vlow, prep->vlow, count * (size_t)kpad * esz,
+                                cudaMemcpyHostToDevice, g->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(g->d_norm, prep->norm, count * 4, cudaMemcpyHostToDevice,
+                                    g->stream);
+            if (e == cudaSuccess && f8) {
+                if ((e = cudaMalloc(&g->d_vscale, rows_pad * 4)) == cudaSuccess &&
+                    (e = cudaMemsetAsync(g->d_vscale, 0, rows_pad * 4, g->stream)) == cudaSuccess)
+                    e = cudaMemcpyAsync(g->d_vscale, prep->scale, count * 4,
+                                        cudaMemcpyHostToDevice, g->stream);
+            }
+            if (e != cudaSuccess) return bail("prepared rows", e);
+        } else if (f8) {
             if ((e = cudaMalloc(&g->d_vscale, rows_pad * 4)) != cudaSuccess)
                 return bail("scales", e);
             if ((e = cudaMemsetAsync(g->d_vscale, 0, rows_pad * 4, g->stream)) != cudaSuccess)
@@ -342,6 +371,59 @@ extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *c
     // the caller's arrays may go once this returns
     if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail("upload", e);
     return g;
+}
+
+}  // namespace
+
+extern "C" FvGpuIndex *fv_gpu_index_upload(const float *vectors, const double *cols,
+                                           const uint32_t *post_rows, const uint32_t *l0,
+                                           uint32_t l0_stride, uint64_t count, int dim,
+                                           int ncols, int device, int precision,
+                                           char *errbuf, size_t errlen) {
+    return upload_impl(vectors, cols, post_rows, l0, l0_stride, count, dim, ncols, device,
+                       precision, nullptr, errbuf, errlen);
+}
+
+extern "C" FvGpuIndex *pv_index_upload_prepared(const float *vectors, const double *cols,
+                                                const uint32_t *post_rows, const uint32_t *l0,
+                                                uint32_t l0_stride, uint64_t count, int dim,
+                                                int ncols, int device, int precision,
+                                                const void *vlow, const float *norms,
+                                                const float *scales, float row_amax,
+                                                char *errbuf, size_t errlen) {
+    const Prepared p{vlow, norms, scales, row_amax};
+    return upload_impl(vectors, cols, post_rows, l0, l0_stride, count, dim, ncols, device,
+                       precision, &p, errbuf, errlen);
+}
+
+extern "C" int64_t pv_index_part_bytes(const FvGpuIndex *g, int part) {
+    if (!g || g->precision == FV_GPU_PREC_FP32 || !g->d_vlow) return -1;
+    const size_t esz = g->precision == FV_GPU_PREC_FP8 ? 1 : 2;
+    switch (part) {
+        case PV_PART_LOWP_ROWS: return (int64_t)(g->count * (size_t)g->kpad * esz);
+        case PV_PART_NORMS: return (int64_t)(g->count * 4);
+        case PV_PART_SCALES: return g->precision == FV_GPU_PREC_FP8 ? (int64_t)(g->count * 4) : -1;
+    }
+    return -1;
+}
+
+extern "C" int pv_index_export(FvGpuIndex *g, int part, void *dst, uint64_t bytes,
+                               float *row_amax, char *errbuf, size_t errlen) {
+    const int64_t need = pv_index_part_bytes(g, part);
+    if (need < 0 || !dst || bytes != (uint64_t)need) {
+        if (errbuf && errlen) snprintf(errbuf, errlen, "export: no such part or wrong size");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(g->mu);
+    PV_CUDA_OK(cudaSetDevice(g->device), errbuf, errlen);
+    const void *src = part == PV_PART_LOWP_ROWS ? g->d_vlow
+                      : part == PV_PART_NORMS  ? (const void *)g->d_norm
+                                               : (const void *)g->d_vscale;
+    PV_CUDA_OK(cudaMemcpyAsync(dst, src, (size_t)need, cudaMemcpyDeviceToHost, g->stream), errbuf,
+               errlen);
+    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    if (row_amax) *row_amax = g->row_amax;
+    return 0;
 }
 
 extern "C" int fv_gpu_mem_probe(uint64_t *free_bytes, uint64_t *total_bytes) {

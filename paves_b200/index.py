@@ -30,7 +30,10 @@ def _err():
 class GpuIndex:
     def __init__(self, vectors: np.ndarray, cols: Optional[np.ndarray] = None,
                  post_rows: Optional[np.ndarray] = None, l0: Optional[np.ndarray] = None,
-                 precision: int = _lib.FV_GPU_PREC_FP32, device: int = -1):
+                 precision: int = _lib.FV_GPU_PREC_FP32, device: int = -1, prepared=None):
+        """prepared: an indexfile.DeviceLayout stored by an earlier upload of
+        these rows at this precision; its low-precision rows, norms and
+        scales are copied to the GPU instead of converted."""
         L = _lib.lib()
         self.vectors = np.ascontiguousarray(vectors, np.float32)
         self.count, self.dim = self.vectors.shape
@@ -48,11 +51,25 @@ class GpuIndex:
             l0 = np.ascontiguousarray(l0, np.uint32)
             l0_stride = l0.shape[1]
         err = _err()
-        h = L.fv_gpu_index_upload(ptr(self.vectors), ptr(self.cols) if self.ncols else None,
-                                  ptr(self.post_rows) if self.ncols else None,
-                                  ptr(l0) if l0 is not None else None, l0_stride,
-                                  self.count, self.dim, self.ncols, device, precision, err,
-                                  len(err))
+        if prepared is not None:
+            if (prepared.precision != precision or prepared.count != self.count
+                    or prepared.dim != self.dim):
+                raise GpuError("stored device layout does not match the rows / precision")
+            rows = np.ascontiguousarray(prepared.rows)
+            norms = np.ascontiguousarray(prepared.norms, np.float32)
+            scales = (None if prepared.scales is None
+                      else np.ascontiguousarray(prepared.scales, np.float32))
+            h = L.pv_index_upload_prepared(
+                ptr(self.vectors), ptr(self.cols) if self.ncols else None,
+                ptr(self.post_rows) if self.ncols else None, ptr(l0) if l0 is not None else None,
+                l0_stride, self.count, self.dim, self.ncols, device, precision, ptr(rows),
+                ptr(norms), ptr(scales), float(prepared.row_amax), err, len(err))
+        else:
+            h = L.fv_gpu_index_upload(ptr(self.vectors), ptr(self.cols) if self.ncols else None,
+                                      ptr(self.post_rows) if self.ncols else None,
+                                      ptr(l0) if l0 is not None else None, l0_stride,
+                                      self.count, self.dim, self.ncols, device, precision, err,
+                                      len(err))
         if not h:
             raise GpuError(err.value.decode())
         self._h = h
@@ -76,6 +93,31 @@ class GpuIndex:
 
     def device(self) -> int:
         return _lib.lib().fv_gpu_index_device(self._h)
+
+    def export_device_layout(self):
+        """This index's low-precision rows, norms and (FP8) scales as an
+        indexfile.DeviceLayout (read back from the GPU)."""
+        from .indexfile import DeviceLayout
+        L = _lib.lib()
+        parts, amax = {}, C.c_float()
+        for part in (_lib.PV_PART_LOWP_ROWS, _lib.PV_PART_NORMS, _lib.PV_PART_SCALES):
+            n = L.pv_index_part_bytes(self._h, part)
+            if n < 0:
+                continue
+            buf = np.empty(n, np.uint8)
+            err = _err()
+            if L.pv_index_export(self._h, part, ptr(buf), n, C.byref(amax), err, len(err)) != 0:
+                raise GpuError(err.value.decode())
+            parts[part] = buf
+        if _lib.PV_PART_LOWP_ROWS not in parts:
+            raise GpuError("an FP32 index has no low-precision layout")
+        esz = 1 if self.precision == _lib.FV_GPU_PREC_FP8 else 2
+        scales = parts.get(_lib.PV_PART_SCALES)
+        return DeviceLayout(self.precision, self.count, self.dim,
+                            parts[_lib.PV_PART_LOWP_ROWS].size // (self.count * esz),
+                            float(amax.value), parts[_lib.PV_PART_LOWP_ROWS],
+                            parts[_lib.PV_PART_NORMS].view(np.float32),
+                            None if scales is None else scales.view(np.float32))
 
     # ------------------------------------------------------------------
     def brute_batch_raw(self, queries: np.ndarray, bp: BatchPred, topb: int):

@@ -155,3 +155,109 @@ def write_index(path: str, vectors: np.ndarray, cols: np.ndarray, M: int, ef_con
         f.flush()
         os.fsync(f.fileno())
     os.replace(tmp, path)
+
+
+# ---------------------------------------------------------------------------
+# Stored device layout: a companion file "<index>.pvdev". The reference
+# reader rejects a file whose size differs from its header's file_size
+# (engine.cpp:274-290), so the device layout lives beside the index file
+# instead of inside it, and the index file stays readable by the engine.
+#
+#   header   magic "PVDEVL01", version, precision, count, dim, kpad,
+#            row_amax, SHA-256 of the index file's header (its section
+#            offsets and file size: a rewritten index makes the companion
+#            stale), section offsets, file size                (128 bytes)
+#   rows     bf16 / fp8 [count][kpad]   (row stride kpad * element size)
+#   norms    f32 [count]
+#   scales   f32 [count]                (FP8 only)
+DEV_MAGIC = b"PVDEVL01"
+DEV_VERSION = 1
+# char[8], u32 version, u32 precision, u64 count, u32 dim, u32 kpad,
+# f32 row_amax, (pad 4), 32s digest, 4 x u64 offsets / size, (pad 24)
+_DEV_HDR = struct.Struct("<8sIIQIIf4x32sQQQQ24x")
+assert _DEV_HDR.size == 128
+PREC_FP8 = 3
+
+
+@dataclass
+class DeviceLayout:
+    precision: int
+    count: int
+    dim: int
+    kpad: int
+    row_amax: float
+    rows: np.ndarray            # u8 [count * kpad * element size]
+    norms: np.ndarray           # f32 [count]
+    scales: Optional[np.ndarray]  # f32 [count] (FP8)
+
+
+def device_layout_path(path: str) -> str:
+    return path + ".pvdev"
+
+
+def _header_digest(path: str) -> bytes:
+    import hashlib
+    with open(path, "rb") as f:
+        return hashlib.sha256(f.read(_HDR.size)).digest()
+
+
+def write_device_layout(path: str, lay: DeviceLayout) -> str:
+    """Writes lay beside the index file `path` (tmp + fsync + rename)."""
+    esz = 1 if lay.precision == PREC_FP8 else 2
+    rows = np.ascontiguousarray(lay.rows, np.uint8).reshape(-1)
+    if rows.size != lay.count * lay.kpad * esz or lay.norms.size != lay.count:
+        raise ValueError("device layout arrays do not match count / kpad")
+    if lay.precision == PREC_FP8 and (lay.scales is None or lay.scales.size != lay.count):
+        raise ValueError("FP8 device layout needs one scale per row")
+    off = _align64(_DEV_HDR.size)
+    off_rows = off; off = _align64(off + rows.size)
+    off_norms = off; off = _align64(off + lay.count * 4)
+    off_scales = off if lay.precision == PREC_FP8 else 0
+    if off_scales:
+        off = _align64(off + lay.count * 4)
+    size = off
+    hdr = _DEV_HDR.pack(DEV_MAGIC, DEV_VERSION, lay.precision, lay.count, lay.dim, lay.kpad,
+                        float(lay.row_amax), _header_digest(path), off_rows, off_norms,
+                        off_scales, size)
+    out = device_layout_path(path)
+    tmp = out + ".tmp"
+    with open(tmp, "wb") as f:
+        f.truncate(size)
+        parts = [(0, np.frombuffer(hdr, np.uint8)), (off_rows, rows),
+                 (off_norms, np.ascontiguousarray(lay.norms, np.float32))]
+        if off_scales:
+            parts.append((off_scales, np.ascontiguousarray(lay.scales, np.float32)))
+        for o, arr in parts:
+            f.seek(o)
+            f.write(arr.tobytes())
+        f.flush()
+        os.fsync(f.fileno())
+    os.replace(tmp, out)
+    return out
+
+
+def read_device_layout(path: str, precision: int) -> Optional[DeviceLayout]:
+    """The stored device layout of index file `path` at `precision`, or None
+    when there is none, it was written for another precision, or the index
+    file was rewritten since (its header digest differs). A companion that
+    claims to match but is malformed raises ValueError."""
+    dp = device_layout_path(path)
+    if not os.path.exists(dp) or os.path.getsize(dp) < _DEV_HDR.size:
+        return None
+    mm = np.memmap(dp, np.uint8, "r")
+    (magic, version, prec, count, dim, kpad, amax, digest, off_rows, off_norms, off_scales,
+     size) = _DEV_HDR.unpack(bytes(mm[:_DEV_HDR.size]))
+    if magic != DEV_MAGIC or version != DEV_VERSION or prec != precision:
+        return None
+    if digest != _header_digest(path):
+        return None
+    if size != os.path.getsize(dp):
+        raise ValueError(f"{dp}: truncated")
+    esz = 1 if prec == PREC_FP8 else 2
+    want = (dim + 127) & ~127 if prec == PREC_FP8 else (dim + 63) & ~63
+    if kpad != want:
+        raise ValueError(f"{dp}: row stride {kpad}, expected {want}")
+    rows = np.frombuffer(mm, np.uint8, count * kpad * esz, off_rows)
+    norms = np.frombuffer(mm, np.float32, count, off_norms)
+    scales = np.frombuffer(mm, np.float32, count, off_scales) if prec == PREC_FP8 else None
+    return DeviceLayout(prec, count, dim, kpad, amax, rows, norms, scales)
