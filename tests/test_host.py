@@ -156,3 +156,33 @@ def test_index_file_roundtrip():
             R = refengine.RefIndex(path)  # the reference engine opens our file
             assert R.graph_entry(vecs[0]) in range(n)
             R.close()
+
+
+def test_identical_predicate_trees_share_one_program():
+    """Batches carry one serialized tree per query; structurally identical
+    trees (any slice of the arrays) compile to one program, as do trees whose
+    compiled programs are equal; distinct ones (down to a constant's bits:
+    -0.0 vs 0.0) stay apart, and a malformed tree is still reported."""
+    import ctypes as C
+    from paves_b200 import _lib, pred
+    L = _lib.lib()
+    P, Cc = 0, 1
+
+    def nprog(preds, ncols=2):
+        bp = pred.concat(preds, 100)
+        err = C.create_string_buffer(256)
+        n = C.c_int()
+        rc = L.pv_pred_check(len(preds), _lib.ptr(bp.qd), _lib.ptr(bp.nodes), len(bp.nodes),
+                             _lib.ptr(bp.children), len(bp.children), _lib.ptr(bp.invals),
+                             len(bp.invals), ncols, C.byref(n), err, 256)
+        return rc, n.value, err.value
+
+    a = pred.And(pred.Cmp(P, "<", 10.0), pred.In(Cc, [3.0, 7.0]))
+    b = pred.Or(pred.Cmp(P, ">", 5.0), pred.Not(pred.In(Cc, [1.0])))
+    assert nprog([a] * 64)[:2] == (0, 1)
+    assert nprog([a, None, b] * 21)[:2] == (0, 2)
+    assert nprog([pred.Cmp(P, "==", 0.0), pred.Cmp(P, "==", -0.0)] * 8)[:2] == (0, 2)
+    # different trees that compile to the same program (one integer set) share it
+    assert nprog([pred.In(Cc, [1.0, 2.0]), pred.In(Cc, [2.0, 1.0])])[:2] == (0, 1)
+    rc, _, msg = nprog([a, pred.Cmp(5, "<", 1.0)])  # column 5 of 2
+    assert rc == -1 and b"column" in msg
