@@ -64,6 +64,9 @@ void pv_batch_free(PvBatch *b);
  * d_queries (nq x dim f32), d_out (nq x topb FvHit) and d_cnt (nq u32) are
  * DEVICE pointers on g's device, allocated by the caller however it may;
  * results have the layout and order of fv_gpu_brute_batch (exact FP32).
+ * The call reads d_queries on the index's own stream, which does not wait
+ * for the caller's streams: the queries must be complete on the device
+ * before the call (e.g. synchronize the stream that wrote them first).
  * Limits: nq <= PV_NOALLOC_MAX_BATCH, topb <= PV_NOALLOC_MAX_TOPB, else -1
  * with a message. The first call on a device looks up the array's device
  * address, so make it before any stream capture. All calls share the array:

@@ -28,6 +28,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <deque>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -137,7 +138,9 @@ struct PvArbiter {
     std::mutex mu;  // wakeups only (data moves through the slot states)
     std::condition_variable wake_worker, wake_backends;
     std::mutex attach_mu;
-    std::vector<Attached> indexes;
+    // a deque: push_back never moves its elements, so the pointer find()
+    // hands the worker stays valid while pv_arbiter_attach adds indexes
+    std::deque<Attached> indexes;
     std::vector<Feedback *> fb;
     pv_arb_exec_fn exec = default_exec;
     void *exec_ctx = nullptr;

@@ -164,14 +164,16 @@ def write_index(path: str, vectors: np.ndarray, cols: np.ndarray, M: int, ef_con
 # instead of inside it, and the index file stays readable by the engine.
 #
 #   header   magic "PVDEVL01", version, precision, count, dim, kpad,
-#            row_amax, SHA-256 of the index file's header (its section
-#            offsets and file size: a rewritten index makes the companion
-#            stale), section offsets, file size                (128 bytes)
+#            row_amax, SHA-256 of the index file's header and vectors
+#            section (the rows the layout is converted from: a rewrite
+#            with other vectors makes the companion stale, even when the
+#            header is byte-identical because count, dim and M are),
+#            section offsets, file size                         (128 bytes)
 #   rows     bf16 / fp8 [count][kpad]   (row stride kpad * element size)
 #   norms    f32 [count]
 #   scales   f32 [count]                (FP8 only)
 DEV_MAGIC = b"PVDEVL01"
-DEV_VERSION = 1
+DEV_VERSION = 2  # 1: digest of the header alone
 # char[8], u32 version, u32 precision, u64 count, u32 dim, u32 kpad,
 # f32 row_amax, (pad 4), 32s digest, 4 x u64 offsets / size, (pad 24)
 _DEV_HDR = struct.Struct("<8sIIQIIf4x32sQQQQ24x")
@@ -195,10 +197,21 @@ def device_layout_path(path: str) -> str:
     return path + ".pvdev"
 
 
-def _header_digest(path: str) -> bytes:
+def _source_digest(path: str) -> bytes:
+    """SHA-256 of the index file's header and its vectors section. The
+    header alone does not identify the rows: node levels come from a hash
+    of the row number (engine.cpp:720-729), so two indexes of the same
+    count, dim and M have byte-identical headers."""
     import hashlib
-    with open(path, "rb") as f:
-        return hashlib.sha256(f.read(_HDR.size)).digest()
+    mm = np.memmap(path, np.uint8, "r")
+    h = _HDR.unpack(bytes(mm[:_HDR.size]))
+    dim, count, off_vec = h[2], h[3], h[42]
+    end = off_vec + int(count) * int(dim) * 4
+    if end > mm.size:
+        raise ValueError(f"index file {path}: vectors section past the end")
+    d = hashlib.sha256(memoryview(mm[:_HDR.size]))
+    d.update(memoryview(mm[off_vec:end]))
+    return d.digest()
 
 
 def write_device_layout(path: str, lay: DeviceLayout) -> str:
@@ -217,7 +230,7 @@ def write_device_layout(path: str, lay: DeviceLayout) -> str:
         off = _align64(off + lay.count * 4)
     size = off
     hdr = _DEV_HDR.pack(DEV_MAGIC, DEV_VERSION, lay.precision, lay.count, lay.dim, lay.kpad,
-                        float(lay.row_amax), _header_digest(path), off_rows, off_norms,
+                        float(lay.row_amax), _source_digest(path), off_rows, off_norms,
                         off_scales, size)
     out = device_layout_path(path)
     tmp = out + ".tmp"
@@ -238,8 +251,9 @@ def write_device_layout(path: str, lay: DeviceLayout) -> str:
 
 def read_device_layout(path: str, precision: int) -> Optional[DeviceLayout]:
     """The stored device layout of index file `path` at `precision`, or None
-    when there is none, it was written for another precision, or the index
-    file was rewritten since (its header digest differs). A companion that
+    when there is none, it was written for another precision or by another
+    version, or the index file was rewritten since (the digest of its
+    header and vectors differs). A companion that
     claims to match but is malformed raises ValueError."""
     dp = device_layout_path(path)
     if not os.path.exists(dp) or os.path.getsize(dp) < _DEV_HDR.size:
@@ -249,7 +263,7 @@ def read_device_layout(path: str, precision: int) -> Optional[DeviceLayout]:
      size) = _DEV_HDR.unpack(bytes(mm[:_DEV_HDR.size]))
     if magic != DEV_MAGIC or version != DEV_VERSION or prec != precision:
         return None
-    if digest != _header_digest(path):
+    if digest != _source_digest(path):
         return None
     if size != os.path.getsize(dp):
         raise ValueError(f"{dp}: truncated")

@@ -277,3 +277,29 @@ def test_stuck_worker_times_out_and_slot_is_reused(ds):
         assert first[0][0] == 1
         # both slots are free again
         assert a.submit(8, 1, PV_STRAT_GPU_BRUTE, ds.queries[1], None, want=5)[0] == 1
+
+
+def test_attach_while_serving_keeps_served_index_valid(ds):
+    """pv_arbiter_attach may run beside the worker: a batch in flight keeps
+    using its index's registration (tids, count) while hundreds of other
+    indexes are attached, which used to reallocate the registry under it."""
+    ex = OracleExec(ds)
+    ex.gate = threading.Event()
+    tids = np.arange(N, dtype=np.uint64) * 3 + 5
+    q = ds.queries[0]
+    with Arbiter(nslots=16, batch_max=8, wait_us=200, idle_us=100) as a:
+        a.set_executor(ex)
+        a.attach(1, 9, count=N, dim=D, tids=tids)
+        out = {}
+        t = threading.Thread(target=lambda: out.setdefault(
+            "r", a.submit(1, 9, PV_STRAT_GPU_BRUTE, q, None, want=10)))
+        t.start()
+        time.sleep(0.05)  # the worker holds the batch at the gate
+        for relid in range(100, 400):
+            a.attach(relid, relid, count=N, dim=D, tids=tids)
+        ex.gate.set()
+        t.join(30)
+        rc, hits, more = out["r"]
+        ids, _ = _truth(ds, q, None, 10)
+        assert rc == 1
+        assert np.array_equal(hits["node"], ids.astype(np.uint64) * 3 + 5)

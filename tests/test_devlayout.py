@@ -59,6 +59,15 @@ def test_fallbacks_and_errors():
         # a rewritten index file (another graph: other offsets) makes it stale
         Hnsw(ds.vectors[:250], 4, 16).write(path, ds.cols[:, :250])
         assert read_device_layout(path, FP8) is None
+        # the same count, dim and M with other vectors: node levels hash the
+        # row number, so the header is byte-identical; the rows are not
+        write_device_layout(path, _layout(FP8, 250, 20, rng))
+        assert read_device_layout(path, FP8) is not None
+        hdr0 = open(path, "rb").read(264)
+        other = np.ascontiguousarray(ds.vectors[:250][::-1])
+        Hnsw(other, 4, 16).write(path, ds.cols[:, :250])
+        assert open(path, "rb").read(264) == hdr0
+        assert read_device_layout(path, FP8) is None
         # matching but truncated
         write_device_layout(path, _layout(FP8, 250, 20, rng))
         dp = device_layout_path(path)

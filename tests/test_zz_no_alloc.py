@@ -56,6 +56,38 @@ def test_noalloc_matches_regular_entry_point_twice(dim):
     gi.close()
 
 
+def test_noalloc_leaves_free_device_memory_unchanged():
+    """The point of the entry point: after its first call on a device,
+    further calls of any allowed shape allocate nothing on the device (the
+    caller's buffers are allocated once, up front, at the largest shape)."""
+    import torch
+    ds = datagen.make_dataset(50_000, 96, nq=32)
+    gi = GpuIndex(ds.vectors, ds.cols, device=0)
+    dev = torch.device(f"cuda:{gi.device()}")
+    L = _lib.lib()
+    err = C.create_string_buffer(256)
+    d_q = torch.from_numpy(np.ascontiguousarray(ds.queries, np.float32)).to(dev)
+    d_out = torch.zeros(32 * 32 * 16, dtype=torch.uint8, device=dev)
+    d_cnt = torch.zeros(32, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def call(nq, topb):
+        rc = L.pv_brute_batch_noalloc(gi.handle, nq, d_q.data_ptr(), topb, d_out.data_ptr(),
+                                      d_cnt.data_ptr(), err, 256)
+        assert rc == 0, err.value.decode()
+
+    call(32, 32)  # first call on the device: looks up the scratch address
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for nq, topb in [(1, 1), (32, 32), (7, 10), (16, 3), (32, 1), (2, 32)]:
+        call(nq, topb)
+        assert torch.cuda.mem_get_info(dev)[0] == free0, (nq, topb)
+    # and the last call's answer is still the regular entry point's
+    out = d_out.cpu().numpy()[:2 * 32 * 16].view(_lib.HIT_DTYPE).reshape(2, 32)
+    r_ids, r_dists, r_cnt, _ = gi.brute_batch(ds.queries[:2], [None, None], 32)
+    assert np.array_equal(out["node"], r_ids) and np.array_equal(out["dist"], r_dists)
+    gi.close()
+
+
 def test_noalloc_rejects_oversize_requests():
     ds = datagen.make_dataset(5000, 64, nq=40)
     gi = GpuIndex(ds.vectors, ds.cols, device=0)
