@@ -19,7 +19,17 @@ filtered L2 top-10. A step is one batch; steps rotate through the classes.
             batch) over its average CUDA-event duration, against
             MEASURED_PEAKS.json
   cpu_baseline  the reference engine's CPU BruteCursor (oracle/_ref, built
-            from the reference sources) on a bounded sample, all host cores
+            from the reference sources) over the 384 queries, all host
+            cores, after one warm-up pass (the method --impl reference
+            repeats per step)
+  parity_vs_reference_cpu  that run's answers against the plain exact
+            path's and the chosen path's: queries with identical ids and
+            identical FP32 distances, at 1M rows
+  reference_gpu  the reference's own CUDA backend (gpu_engine.cu built for
+            sm_100a, oracle/_ref) on the same index, batches and filters,
+            fp32 and sq8, through the engine's batch call with host buffers
+            (a subprocess): e2e queries/s, its profiler's kernel time, and
+            its answers against the reference CPU's
 
 --impl reference times that reference CPU path alone (rank 0).
 Multi-GPU (torchrun): each rank serves its own batches on its own GPU
@@ -126,49 +136,68 @@ ROUTER_FILE = os.path.join(ROOT, "paves_b200", "router_1m128.npz")
 
 
 # ---------------------------------------------------------------- reference CPU
-def reference_cpu_qps(ds, preds, budget_s=20.0, threads=None):
+def write_brute_index(ds, path):
+    """The rows and attribute columns as a PAVES index file (a one-neighbour
+    level 0: the brute paths read no graph)."""
+    from paves_b200.indexfile import write_index
+    n = ds.vectors.shape[0]
+    l0 = np.zeros((n, 3), np.uint32)
+    write_index(path, ds.vectors, ds.cols, 1, 1, np.zeros(n, np.uint8), l0,
+                np.zeros(n + 1, np.uint64), np.zeros(0, np.uint32), 0, 0)
+
+
+def reference_cpu_qps(path, ds, preds, budget_s=20.0, threads=None, keep=False):
     """Reference engine BruteCursor (built from the reference sources), one
     query at a time with `threads` workers, over up to len(preds) queries
-    within budget_s. Returns (qps, queries_run, threads, kind)."""
+    within budget_s. Returns (qps, queries_run, threads, answers) with
+    answers[q] = (ids, dists) when keep."""
     from oracle import refengine
-    from paves_b200.indexfile import write_index
     threads = threads or os.cpu_count() or 1
-    n = ds.vectors.shape[0]
-    with tempfile.TemporaryDirectory(dir="/tmp") as td:
-        path = os.path.join(td, "bench.idx")
-        l0 = np.zeros((n, 3), np.uint32)  # no graph needed for the brute path (M=1)
-        write_index(path, ds.vectors, ds.cols, 1, 1, np.zeros(n, np.uint8), l0,
-                    np.zeros(n + 1, np.uint64), np.zeros(0, np.uint32), 0, 0)
-        R = refengine.RefIndex(path)
-        handles = {}
-        done = 0
-        t0 = time.perf_counter()
-        for q, p in enumerate(preds):
-            key = id(p)
-            if key not in handles:
-                handles[key] = R.compile(p)
-            R.brute(ds.queries[q], handles[key], TOPK, threads=threads)
-            done += 1
-            if time.perf_counter() - t0 > budget_s:
-                break
-        dt = time.perf_counter() - t0
-        for h in handles.values():
-            R.free_pred(h)
-        R.close()
-    return done / dt, done, threads
+    R = refengine.RefIndex(path)
+    handles = {}
+    answers = {}
+    done = 0
+    t0 = time.perf_counter()
+    for q, p in enumerate(preds):
+        key = id(p)
+        if key not in handles:
+            handles[key] = R.compile(p)
+        res = R.brute(ds.queries[q], handles[key], TOPK, threads=threads)
+        if keep:
+            answers[q] = res
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    for h in handles.values():
+        R.free_pred(h)
+    R.close()
+    return done / dt, done, threads, answers
+
+
+def reference_cpu_leg(path, ds, preds, warmup, steps, keep=False):
+    """The CPU baseline both arms report: `warmup` untimed passes over 8
+    queries, then `steps` timed passes over the workload's queries (10 s
+    budget each); the median pass. Returns (qps, queries per pass, threads,
+    answers of the last pass)."""
+    for _ in range(warmup):
+        reference_cpu_qps(path, ds, preds[:8], budget_s=5.0)
+    per, ans, nrun, threads = [], {}, 0, 1
+    for i in range(steps):
+        qps, nrun, threads, ans = reference_cpu_qps(path, ds, preds, budget_s=10.0,
+                                                    keep=keep and i == steps - 1)
+        per.append(qps)
+    return float(np.median(per)), nrun, threads, ans
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     ds, _, preds = make_workload()
-    per_step = []
-    for _ in range(args.warmup):
-        reference_cpu_qps(ds, preds[:8], budget_s=5.0)
-    for _ in range(args.steps):
-        qps, nrun, threads = reference_cpu_qps(ds, preds, budget_s=10.0)
-        per_step.append(qps)
-    qps = float(np.median(per_step))
+    with tempfile.TemporaryDirectory(dir="/tmp") as td:
+        path = os.path.join(td, "bench.idx")
+        write_brute_index(ds, path)
+        qps, nrun, threads, _ = reference_cpu_leg(path, ds, preds, args.warmup, args.steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(qps, 2), "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -179,11 +208,48 @@ def run_reference(args, rank, world):
                    "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK},
         "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
                          "kind": "reference",
-                         "sample": f"up to {BATCH} queries per step, one at a time"},
+                         "sample": f"{nrun} queries (the six class batches) per step, one at "
+                                   "a time; median of the steps"},
         "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(path, ds, classes, steps, precisions=(0, 1), timeout=600):
+    """The reference's own CUDA backend (gpu_engine.cu built for sm_100a,
+    oracle/_ref/libpaves_ref_gpu.so) on the same index, batches and filters,
+    through the engine's batch call with host buffers, in a subprocess
+    (oracle/refgpu.py). Per precision (0 = fp32 exact, 1 = sq8): e2e
+    queries/s, the kernel time its own profiler reports, and the answers."""
+    from oracle import refengine
+    if not refengine.available("gpu"):
+        return {"unavailable": "oracle/_ref/libpaves_ref_gpu.so not built"}, {}
+    td = os.path.dirname(path)
+    qf = os.path.join(td, "queries.npy")
+    cf = os.path.join(td, "classes.json")
+    np.save(qf, ds.queries[:BATCH * len(classes)])
+    with open(cf, "w") as f:
+        json.dump([[n, pred.to_json(p)] for n, p in classes], f)
+    out, answers = {}, {}
+    for prec in precisions:
+        name = {0: "fp32", 1: "sq8"}[prec]
+        of = os.path.join(td, f"ref_{name}.npz")
+        cmd = [sys.executable, "-m", "oracle.refgpu", "brute", "--index", path, "--queries", qf,
+               "--classes", cf, "--batch", str(BATCH), "--topb", str(TOPK), "--precision",
+               str(prec), "--steps", str(max(steps, len(classes))), "--out", of]
+        try:
+            r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=timeout)
+            if r.returncode != 0:
+                out[name] = {"failed": (r.stderr or r.stdout).strip().splitlines()[-1:]}
+                continue
+            out[name] = json.loads(r.stdout.strip().splitlines()[-1])
+            z = np.load(of)
+            answers[name] = {int(k.split("_")[1]): (z[k], z[f"cnt_{k.split('_')[1]}"])
+                             for k in z.files if k.startswith("ids_")}
+        except Exception as e:  # informative only
+            out[name] = {"failed": str(e)}
+    return out, answers
 
 
 # ---------------------------------------------------------------- ours
@@ -437,6 +503,57 @@ def shared_graph(vectors, rank, dist, cache):
     return h
 
 
+def parity_vs_reference(ans, exact, results):
+    """Answers of the reference CPU BruteCursor (query c * BATCH + i of class
+    c) against the plain exact FP32 path and the chosen path: queries whose
+    ids, and whose FP32 distances, are identical."""
+    out = {}
+    for name, get in (("exact_fp32", lambda c: (exact[c][0], exact[c][1], exact[c][2])),
+                      ("chosen", lambda c: (results[c][0], results[c][4], results[c][1]))):
+        n = ids_eq = d_eq = 0
+        for c in range(len(exact)):
+            if name == "chosen" and c not in results:
+                continue
+            ids, dists, cnt = get(c)
+            for i in range(BATCH):
+                q = c * BATCH + i
+                if q not in ans:
+                    continue
+                r_ids, r_d = ans[q]
+                k = int(cnt[i])
+                n += 1
+                same = k == len(r_ids) and np.array_equal(ids[i, :k].astype(np.uint64), r_ids)
+                ids_eq += int(same)
+                d_eq += int(same and np.array_equal(dists[i, :k], r_d))
+        out[name] = {"queries": n, "ids_equal": ids_eq, "dist_equal": d_eq}
+    return out
+
+
+def summarize_ref_gpu(rg, rg_ans, cpu_ans):
+    """The reference GPU leg's numbers, with its answers checked against the
+    reference CPU's (fp32: identical ids; sq8: recall@10)."""
+    for name, per in rg_ans.items():
+        if name not in rg or "failed" in rg[name]:
+            continue
+        n = eq = 0
+        rec = []
+        for c, (ids, cnt) in per.items():
+            for i in range(ids.shape[0]):
+                q = c * BATCH + i
+                if q not in cpu_ans:
+                    continue
+                r_ids = cpu_ans[q][0]
+                k = int(cnt[i])
+                n += 1
+                eq += int(k == len(r_ids) and np.array_equal(ids[i, :k].astype(np.uint64), r_ids))
+                if len(r_ids):
+                    rec.append(np.isin(r_ids, ids[i, :k]).mean())
+        rg[name]["vs_reference_cpu"] = {"queries": n, "ids_equal": eq,
+                                        "recall_at_10": round(float(np.mean(rec)), 4)
+                                        if rec else None}
+    return rg
+
+
 def reduce_max(vals, dist, device):
     """Element-wise max over ranks (the job's time is its slowest rank's)."""
     if not dist:
@@ -453,7 +570,10 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the baseline legs (reference CPU, reference GPU, parity)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference GPU leg")
     ap.add_argument("--workload", default="headline", choices=["headline", "stream", "graph"],
                     help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency); "
                          "graph: filtered HNSW search at ef 32..256 beside the reference cursor")
@@ -561,7 +681,7 @@ def main():
         st_sum += st
         launches += int(L.pv_last_launches(gi.handle))
         graph_steps += ex
-        results[c] = (ids, cnt, dec, ex)
+        results[c] = (ids, cnt, dec, ex, dists)
     wall_s = time.perf_counter() - t0
     clocks = clk.stop()
     barrier()
@@ -573,7 +693,7 @@ def main():
     for c, (name, *_rest) in enumerate(cls):
         if c not in results:
             continue
-        ids, cnt, dec, ex = results[c]
+        ids, cnt, dec, ex, _ = results[c]
         xi, _, xc, _ = exact[c]
         r = [np.isin(xi[i, :xc[i]], ids[i, :cnt[i]]).sum() / max(1, int(xc[i]))
              for i in range(BATCH)]
@@ -620,17 +740,25 @@ def main():
     h2d = q.nbytes + bp.qd.nbytes + bp.nodes.nbytes + bp.children.nbytes + bp.invals.nbytes
     d2h = BATCH * TOPK * 16 + BATCH * 4 + BATCH * 2
 
-    cpu = None
+    cpu, parity, ref_gpu = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import refengine
-            if refengine.available("cpu"):
-                qps, nrun_c, threads = reference_cpu_qps(ds, preds_all, budget_s=15.0)
-                cpu = {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
-                       "kind": "reference",
-                       "sample": f"{nrun_c} queries of the six class batches, one at a time "
-                                 "(BruteCursor)"}
-        except Exception as e:  # baseline is informative only
+            with tempfile.TemporaryDirectory(dir="/tmp") as td:
+                path = os.path.join(td, "bench.idx")
+                write_brute_index(ds, path)
+                if refengine.available("cpu"):
+                    qps, nrun_c, threads, ans = reference_cpu_leg(path, ds, preds_all, 1, 1,
+                                                                  keep=True)
+                    cpu = {"value": round(qps, 2), "unit": "queries/s", "cores": threads,
+                           "kind": "reference",
+                           "sample": f"{nrun_c} queries (the six class batches), one at a "
+                                     "time (BruteCursor), after one warm-up pass"}
+                    parity = parity_vs_reference(ans, exact, results)
+                if not args.no_ref_gpu:
+                    rg, rg_ans = reference_gpu_leg(path, ds, classes, args.steps)
+                    ref_gpu = summarize_ref_gpu(rg, rg_ans, ans if cpu else {})
+        except Exception as e:  # baselines are informative only
             cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"failed: {e}"}
 
@@ -665,6 +793,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(achieved / hbm, 4),
                          "traffic": load_traffic("scan_tc_kernel"),
+                         "traffic_source": "ncu capture of the same kernel and workload "
+                                           "(profiles/traffic.json), not this run",
                          "kernel": "scan_tc_kernel", "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": round(scan_ms, 4)},
             "scan_gbs_batch1": round(scan_gbs_b1, 1),
@@ -677,6 +807,8 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "cpu_baseline": cpu,
+            "parity_vs_reference_cpu": parity,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     router.close()

@@ -345,6 +345,10 @@ FvGpuIndex *pv_index_upload_prepared(const float *vectors, const double *cols,
  * (1 = always when the index has 8+ tiles per CTA, 2 = never; the main
  * pass then bounds itself from its own lists). -1: bad value. */
 int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, int seed);
+/* on = 1: later reduced-precision batches on g re-rank 4 x topb candidates
+ * even when the BF16 distances are certified exact (the superset that
+ * inexact distances need); 0 restores the certified width. -1: bad value. */
+int pv_tc_wide_superset(FvGpuIndex *g, int on);
 int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,
                     uint64_t *bound, char *errbuf, size_t errlen);

@@ -207,3 +207,67 @@ class RefIndex:
     def graph_entry(self, q):
         q = np.ascontiguousarray(q, np.float32)
         return int(self.L.fv_index_graph_entry(self.h, q.ctypes.data))
+
+    # -- the engine's GPU batch calls (kind "gpu": the reference's own CUDA
+    # backend; kind "dropin": the same engine over libpaves_gpu.so)
+    def serialize(self, pred_h):
+        """fv_pred_serialize (engine.cpp:1168-1224) of a compiled predicate
+        into owned buffers: (FvGpuBatchPred, buffers, total_rows). None =
+        no filter."""
+        bp = FvGpuBatchPred()
+        total = C.c_uint64(0)
+        if pred_h is None:
+            return bp, [], None
+        nodes = np.zeros(48 * 40, np.uint8)
+        children = np.zeros(96, np.int32)
+        invals = np.zeros(128, np.float64)
+        spans = np.zeros(4096 * 12, np.uint8)
+        rc = self.L.fv_pred_serialize(self.h, pred_h, nodes.ctypes.data, 48,
+                                      children.ctypes.data, 96, invals.ctypes.data, 128,
+                                      spans.ctypes.data, 4096, C.byref(bp), C.byref(total))
+        if rc != 0:
+            raise RuntimeError("fv_pred_serialize: capacity exceeded")
+        return bp, [nodes, children, invals, spans], int(total.value)
+
+    def gpu_precision(self, precision, device=-1):
+        """Sets the upload precision (0 fp32, 1 sq8) and uploads."""
+        self.L.fv_engine_gpu_precision(int(precision))
+        if self.L.fv_index_gpu_ensure(self.h, int(device)) != 0:
+            raise RuntimeError("fv_index_gpu_ensure failed")
+
+    def gpu_brute_batch(self, queries, bps, topb):
+        """fv_gpu_exec_brute_batch (engine.cpp:1290-1313): bps one
+        FvGpuBatchPred per query. Returns (ids, dists, cnt, truncated)."""
+        q = np.ascontiguousarray(queries, np.float32)
+        nq = q.shape[0]
+        arr = (FvGpuBatchPred * nq)(*bps)
+        out = (FvHit * (nq * topb))()
+        cnt = np.zeros(nq, np.uint32)
+        tr = np.zeros(nq, np.uint8)
+        rc = self.L.fv_gpu_exec_brute_batch(self.h, nq, q.ctypes.data, arr, topb, out,
+                                             cnt.ctypes.data, tr.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("fv_gpu_exec_brute_batch failed")
+        hits = np.frombuffer(out, np.dtype({"names": ["node", "dist"], "formats": ["<u8", "<f4"],
+                                            "offsets": [0, 8], "itemsize": 16}))
+        hits = hits.reshape(nq, topb)
+        return hits["node"].copy(), hits["dist"].copy(), cnt, tr
+
+    def gpu_graph_batch(self, queries, entries, bps, ef, max_visited):
+        """fv_gpu_exec_graph_batch (engine.cpp:1315-1339). Returns (ids,
+        dists, cnt, exhausted)."""
+        q = np.ascontiguousarray(queries, np.float32)
+        nq = q.shape[0]
+        ent = np.ascontiguousarray(entries, np.uint32)
+        arr = (FvGpuBatchPred * nq)(*bps)
+        out = (FvHit * (nq * ef))()
+        cnt = np.zeros(nq, np.uint32)
+        ex = np.zeros(nq, np.uint8)
+        rc = self.L.fv_gpu_exec_graph_batch(self.h, nq, q.ctypes.data, ent.ctypes.data, arr, ef,
+                                            max_visited, out, cnt.ctypes.data, ex.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("fv_gpu_exec_graph_batch failed")
+        hits = np.frombuffer(out, np.dtype({"names": ["node", "dist"], "formats": ["<u8", "<f4"],
+                                            "offsets": [0, 8], "itemsize": 16}))
+        hits = hits.reshape(nq, ef)
+        return hits["node"].copy(), hits["dist"].copy(), cnt, ex

@@ -204,6 +204,13 @@ extern "C" int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, in
     return 0;
 }
 
+extern "C" int pv_tc_wide_superset(FvGpuIndex *g, int on) {
+    if (!g || on < 0 || on > 1) return -1;
+    std::lock_guard<std::mutex> lk(g->mu);
+    g->force_wide_superset = on;
+    return 0;
+}
+
 extern "C" int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                                const int32_t *children, int nchildren, const double *invals,
                                int ninvals, uint64_t *bound, char *errbuf, size_t errlen) {

@@ -116,6 +116,7 @@ struct FvGpuIndex {
     // tensor-core scan shape overrides (0 = built-in choice): epilogue warp
     // groups, pipeline stages, CTAs along the rows per query tile
     int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0, tune_seed = 0;
+    int force_wide_superset = 0;  // re-rank 4 x topb even when BF16 is certified exact
     // encoded TMA descriptors of the tensor-core scan (CUtensorMap, 128 B):
     // the rows' (fixed after upload) and the staged queries' (re-encoded
     // when their buffer or row count changes)

@@ -924,8 +924,8 @@ static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner,
 // sums below 2^24), since then the scan's top-k already is the exact top-k.
 // 0 = topb too large.
 int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax) {
-    const bool exact =
-        g->precision != FV_GPU_PREC_FP8 && pv_bf16_exact(g->dim, g->row_amax, q_amax);
+    const bool exact = g->precision != FV_GPU_PREC_FP8 && !g->force_wide_superset &&
+                       pv_bf16_exact(g->dim, g->row_amax, q_amax);
     const int s = exact ? (int)topb : 4 * (int)topb;
     return s <= TC_MAX_SUPERSET ? s : 0;  // 0: topb beyond the superset capacity
 }

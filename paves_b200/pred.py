@@ -83,6 +83,33 @@ class Not(Pred):
         return f"Not({self.children[0]!r})"
 
 
+def to_json(p: Optional[Pred]):
+    """A JSON-able nested list form of a tree (None = no filter)."""
+    if p is None:
+        return None
+    if isinstance(p, Cmp):
+        return ["cmp", p.col, p.op, p.value]
+    if isinstance(p, In):
+        return ["in", p.col, list(p.values)]
+    kind = {And: "and", Or: "or", Not: "not"}[type(p)]
+    return [kind] + [to_json(c) for c in p.children]
+
+
+def from_json(j) -> Optional[Pred]:
+    """Inverse of to_json."""
+    if j is None:
+        return None
+    k = j[0]
+    if k == "cmp":
+        return Cmp(int(j[1]), j[2], float(j[3]))
+    if k == "in":
+        return In(int(j[1]), j[2])
+    kids = [from_json(c) for c in j[1:]]
+    if k == "not":
+        return Not(kids[0])
+    return (And if k == "and" else Or)(*kids)
+
+
 @dataclass
 class Serialized:
     nodes: np.ndarray     # NODE_DTYPE
