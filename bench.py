@@ -424,8 +424,10 @@ def graph_bench(args):
     """Filtered graph search: the 1M x 128 set, HNSW (M=16, efConstruction
     200) built by the library, 64 queries per batch, filters at 1%, 10% and
     50%, ef in {32, 64, 128, 256}; recall@10 against the exact scan and
-    device-time QPS, beside the reference engine's HnswCursor (built from
-    its sources) on the same graph file, one query per host thread."""
+    device-time and wall-clock (host buffers) QPS, beside the reference
+    engine's HnswCursor (built from its sources) on the same graph file, one
+    query per host thread, and the reference's own GPU graph kernel through
+    the engine's batch call (wall clock, host buffers)."""
     from concurrent.futures import ThreadPoolExecutor
     ds, _, _ = make_workload()
     cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
@@ -443,9 +445,11 @@ def graph_bench(args):
                 gi.graph_batch(q, ent, preds, ef)
             dev = 0.0
             reps = max(1, min(args.steps, 10))
+            t0 = time.perf_counter()
             for _ in range(reps):
                 ids, _, cnt, _ = gi.graph_batch(q, ent, preds, ef)
                 dev += L.pv_last_kernel_ms(gi.handle)
+            wall = time.perf_counter() - t0
             rec = float(np.mean([np.isin(xi[i, :xc[i]], ids[i, :TOPK]).sum() / max(1, int(xc[i]))
                                  for i in range(BATCH)]))
             st = np.zeros(BATCH * 4, np.uint32)
@@ -453,6 +457,7 @@ def graph_bench(args):
             st = st.reshape(BATCH, 4)
             res.append({"filter": name, "ef": ef, "recall_at_10": round(rec, 4),
                         "qps": round(BATCH * reps / (dev / 1e3), 1),
+                        "qps_e2e": round(BATCH * reps / wall, 1),
                         "mean_steps": round(float(st[:, 0].mean()), 1),
                         "mean_visited": round(float(st[:, 1].mean()), 1)})
     ref = []
@@ -479,15 +484,133 @@ def graph_bench(args):
             R.close()
     except Exception as e:  # the reference arm is informative only
         ref = [{"failed": str(e)}]
+    # the reference's own GPU graph kernel (fv_graph_kernel, gpu_engine.cu
+    # built for sm_100a) on the same graph file, entries and filters
+    ref_gpu = []
+    try:
+        from oracle import refengine
+        if refengine.available("gpu") and not args.no_ref_gpu:
+            td = tempfile.mkdtemp(dir="/tmp")
+            path = os.path.join(td, "graph.idx")
+            h.write(path, ds.cols)
+            qf, cf, of = (os.path.join(td, x) for x in ("q.npy", "c.json", "ids.npz"))
+            np.save(qf, q)
+            gp = list(datagen.graph_predicates().items())
+            with open(cf, "w") as f:
+                json.dump([[n, pred.to_json(p)] for n, p in gp], f)
+            cmd = [sys.executable, "-m", "oracle.refgpu", "graph", "--index", path, "--queries",
+                   qf, "--classes", cf, "--batch", str(BATCH), "--k", str(TOPK), "--ef",
+                   "32,64,128,256", "--steps", str(max(1, min(args.steps, 10))), "--out", of]
+            r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+            if r.returncode != 0:
+                ref_gpu = [{"failed": (r.stderr or r.stdout).strip().splitlines()[-1:]}]
+            else:
+                rl = json.loads(r.stdout.strip().splitlines()[-1])
+                z = np.load(of)
+                for e in rl["results"]:
+                    p = dict(gp)[e["filter"]]
+                    xi, _, xc, _ = gi.brute_batch(q, [p] * BATCH, TOPK)
+                    ids = z[f"{e['filter']}_{e['ef']}_ids"]
+                    cnt = z[f"{e['filter']}_{e['ef']}_cnt"]
+                    e["recall_at_10"] = round(float(np.mean(
+                        [np.isin(xi[i, :xc[i]], ids[i, :cnt[i]]).sum() / max(1, int(xc[i]))
+                         for i in range(BATCH)])), 4)
+                    ref_gpu.append(e)
+            for f in (path, qf, cf, of):
+                if os.path.exists(f):
+                    os.unlink(f)
+            os.rmdir(td)
+    except Exception as e:
+        ref_gpu = [{"failed": str(e)}]
     line = {"metric": "filtered graph search QPS, 1M x 128 L2, HNSW level 0", "unit": "queries/s",
             "value": max(r["qps"] for r in res), "higher_is_better": True, "n_gpus": 1,
             "data": "synthetic",
             "config": {"workload": "1M x 128 Gaussian-mixture rows, HNSW M=16 efC=200 built by "
                                    "the library, 64-query batches, filters 1%/10%/50%, top-10",
                        "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK},
-            "results": res, "reference_cpu": ref}
+            "results": res, "reference_cpu": ref, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
     gi.close()
+
+
+def batches_bench(args):
+    """Batch sizes 1, 64, 512 and 4096 on the 1M x 128 set, filters rotating
+    per query through the six classes, top-10: this library through
+    fv_gpu_brute_batch with host buffers (exact FP32 upload, and BF16 upload
+    = tensor-core scan + exact re-rank), calls of at most 1024 queries
+    (FV_GPU_MAX_BATCH), wall clock; beside the reference's own CUDA backend
+    (oracle/_ref, fp32 and sq8) driven the same way in a subprocess. Also
+    this library's device time per batch (prepared, resident inputs)."""
+    ds, classes, _ = make_workload(nb=4096 // 6 + 1)
+    nq_all = 4096
+    preds = [classes[q % len(classes)][1] for q in range(nq_all)]
+    sizes = [1, 64, 512, 4096]
+    out = {"ours": {}, "reference_gpu": {}}
+    reps = {1: 60, 64: 30, 512: 8, 4096: 3}
+    for prec, name in ((_lib.FV_GPU_PREC_FP32, "fp32"), (_lib.FV_GPU_PREC_BF16, "bf16")):
+        gi = GpuIndex(ds.vectors, ds.cols, precision=prec)
+        res = {}
+        for B in sizes:
+            q = ds.queries[:B]
+
+            def call():
+                for s0 in range(0, B, 1024):
+                    gi.brute_batch(q[s0:s0 + 1024], preds[s0:min(B, s0 + 1024)], TOPK)
+
+            for _ in range(2):
+                call()
+            t0 = time.perf_counter()
+            for _ in range(reps[B]):
+                call()
+            wall = (time.perf_counter() - t0) / reps[B]
+            bp = pred.concat(preds[:B], N_ROWS)
+            b = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_EXACT if prec ==
+                               _lib.FV_GPU_PREC_FP32 else _lib.PV_MODE_LOW)
+            batch_run(b, 2)
+            ms, _ = batch_run(b, reps[B])
+            _lib.lib().pv_batch_free(b)
+            res[str(B)] = {"qps_e2e": round(B / wall, 1), "ms_e2e": round(1e3 * wall, 3),
+                           "qps_device": round(B * reps[B] / (ms / 1e3), 1),
+                           "ms_device": round(ms / reps[B], 4)}
+        out["ours"][name] = res
+        gi.close()
+    from oracle import refengine
+    if refengine.available("gpu") and not args.no_ref_gpu:
+        td = tempfile.mkdtemp(dir="/tmp")
+        path = os.path.join(td, "b.idx")
+        write_brute_index(ds, path)
+        qf, cf = os.path.join(td, "q.npy"), os.path.join(td, "c.json")
+        np.save(qf, ds.queries[:nq_all])
+        with open(cf, "w") as f:
+            json.dump([[n, pred.to_json(p)] for n, p in classes], f)
+        for prec, name in ((0, "fp32"), (1, "sq8")):
+            res = {}
+            for B in sizes:
+                cmd = [sys.executable, "-m", "oracle.refgpu", "brute", "--index", path,
+                       "--queries", qf, "--classes", cf, "--batch", str(B), "--topb", str(TOPK),
+                       "--precision", str(prec), "--steps", str(reps[B]), "--mixed"]
+                try:
+                    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True,
+                                       timeout=900)
+                    if r.returncode != 0:
+                        res[str(B)] = {"failed": (r.stderr or r.stdout).strip().splitlines()[-1:]}
+                        continue
+                    rl = json.loads(r.stdout.strip().splitlines()[-1])
+                    res[str(B)] = {"qps_e2e": rl["qps_e2e"],
+                                   "kernel_ms_per_call": rl["kernel_ms_per_call"]}
+                except Exception as e:
+                    res[str(B)] = {"failed": str(e)}
+            out["reference_gpu"][name] = res
+        for f in (path, qf, cf):
+            os.unlink(f)
+        os.rmdir(td)
+    line = {"metric": "filtered top-10 QPS by batch size, 1M x 128 L2", "unit": "queries/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "1M x 128 Gaussian-mixture rows, filters rotating per query "
+                                   "through the six classes, top-10; calls of <= 1024 queries",
+                       "rows": N_ROWS, "dim": DIM, "k": TOPK, "batches": sizes},
+            "results": out}
+    print(json.dumps(line), flush=True)
 
 
 def shared_graph(vectors, rank, dist, cache):
@@ -574,9 +697,11 @@ def main():
                     help="skip the baseline legs (reference CPU, reference GPU, parity)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference GPU leg")
-    ap.add_argument("--workload", default="headline", choices=["headline", "stream", "graph"],
+    ap.add_argument("--workload", default="headline",
+                    choices=["headline", "stream", "graph", "batches"],
                     help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency); "
-                         "graph: filtered HNSW search at ef 32..256 beside the reference cursor")
+                         "graph: filtered HNSW search at ef 32..256 beside the reference cursor; "
+                         "batches: batch sizes 1..4096 beside the reference GPU kernels")
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES),
                     help="run one batch shape --steps times and exit (for profilers)")
     ap.add_argument("--tc-shape", default=None,
@@ -588,6 +713,9 @@ def main():
         return
     if args.workload == "graph":
         graph_bench(args)
+        return
+    if args.workload == "batches":
+        batches_bench(args)
         return
     if args.kernel_case:
         shape = None
