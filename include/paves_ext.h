@@ -349,6 +349,12 @@ int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, int seed);
  * even when the BF16 distances are certified exact (the superset that
  * inexact distances need); 0 restores the certified width. -1: bad value. */
 int pv_tc_wide_superset(FvGpuIndex *g, int on);
+/* Limit (ns, at most 10 s; 0 = the default 2 s) after which a wait of the
+ * tensor-core scan gives up: the kernel records which role gave up, waits
+ * (up to 2 s, whatever this limit) for the copies and MMAs it issued,
+ * frees its tensor memory and returns, and the batch call returns -1 with
+ * "wait expired" in errbuf; the index stays usable. -1: bad value. */
+int pv_tc_timeout(FvGpuIndex *g, uint64_t ns);
 int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,
                     uint64_t *bound, char *errbuf, size_t errlen);

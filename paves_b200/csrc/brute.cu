@@ -147,7 +147,10 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     g->tc_unc = nullptr;
 
     ScanPlan pl;
-    if (!plan_scan_f32(g->count, g->dpad, nq, (int)topb, g->sm_count, pl)) {
+    // query tiles of 32-64 take the register-blocked kernel (FP32-pipe
+    // bound), small tiles the bandwidth-bound one
+    const bool tiled = plan_scan_f32t(g->count, g->dpad, nq, (int)topb, g->sm_count, pl);
+    if (!tiled && !plan_scan_f32(g->count, g->dpad, nq, (int)topb, g->sm_count, pl)) {
         snprintf(errbuf, errlen, "gpu: dimension %d not supported by the scan", g->dim);
         return -1;
     }
@@ -176,7 +179,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     a.part_cnt = s.part_cnt.as<uint32_t>();
     if (ev) cudaEventRecord(ev[1], g->stream);
     g->launches += 2;  // scan + merge
-    PV_CUDA_OK(launch_scan_f32(a, pl, g->stream), errbuf, errlen);
+    PV_CUDA_OK(tiled ? launch_scan_f32t(a, pl, g->stream) : launch_scan_f32(a, pl, g->stream),
+               errbuf, errlen);
     if (ev) {
         cudaEventRecord(ev[2], g->stream);
         cudaEventRecord(ev[3], g->stream);

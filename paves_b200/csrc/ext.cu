@@ -204,6 +204,13 @@ extern "C" int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, in
     return 0;
 }
 
+extern "C" int pv_tc_timeout(FvGpuIndex *g, uint64_t ns) {
+    if (!g || ns > 10000000000ull) return -1;
+    std::lock_guard<std::mutex> lk(g->mu);
+    g->tc_timeout_ns = ns;
+    return 0;
+}
+
 extern "C" int pv_tc_wide_superset(FvGpuIndex *g, int on) {
     if (!g || on < 0 || on > 1) return -1;
     std::lock_guard<std::mutex> lk(g->mu);

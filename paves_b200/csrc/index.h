@@ -117,6 +117,7 @@ struct FvGpuIndex {
     // groups, pipeline stages, CTAs along the rows per query tile
     int tune_epi = 0, tune_ns = 0, tune_grow = 0, tune_rep = 0, tune_seed = 0;
     int force_wide_superset = 0;  // re-rank 4 x topb even when BF16 is certified exact
+    uint64_t tc_timeout_ns = 0;   // tensor-core scan wait limit (0: 2 s)
     // encoded TMA descriptors of the tensor-core scan (CUtensorMap, 128 B):
     // the rows' (fixed after upload) and the staged queries' (re-encoded
     // when their buffer or row count changes)

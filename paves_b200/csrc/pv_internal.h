@@ -75,6 +75,10 @@ int scan_f32_max_qt(int dim);
 bool plan_scan_f32(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPlan &pl,
                    uint64_t min_rows = 2048);
 cudaError_t launch_scan_f32(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st);
+// register-blocked exact scan for query tiles of 32 / 64 (scan_f32t.cu):
+// false when the batch is too small, K > 64 or dpad > 256
+bool plan_scan_f32t(uint64_t nrows, int dpad, int nq, int K, int sm_count, ScanPlan &pl);
+cudaError_t launch_scan_f32t(const ScanF32Args &a, const ScanPlan &pl, cudaStream_t st);
 cudaError_t launch_merge(const uint64_t *part, const uint32_t *part_cnt, int grow, int K,
                          const ScanPlan &pl, const unsigned long long *tau,
                          const int32_t *qprog, const unsigned long long *popcnt,

@@ -57,6 +57,8 @@ constexpr int TC_KBS = 2;           // K-blocks per pipeline stage
 constexpr int TC_MAX_SUPERSET = 1024;
 constexpr int TC_MAX_LIST = 64;
 constexpr int TC_MAX_STAGES = 8;   // TMA pipeline stages at most
+constexpr int TC_NR = 8;            // tiles of row norms in flight (shared-memory ring)
+constexpr int TC_NSLOT_F = 2 * TC_BN;  // floats per norm slot: norms, then fp8 scales
 
 template <bool FP8>
 __device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
@@ -96,7 +98,11 @@ struct TcArgs {
     // [nq] smallest last key of a full list (the merge's certificate), or null
     unsigned long long *fullmin;
     int *err;
+    // waits give up after timeout_ns (the kernel then sets *err and
+    // unwinds); once unwinding, it still waits up to drain_ns for the copies
+    // and MMAs it issued, so none is in flight when the CTA leaves
     uint64_t timeout_ns;
+    uint64_t drain_ns;
     // optional per-tile timestamps of CTA 0 (globaltimer ns):
     // [t][0] stage issued, [t][1] MMA issued, [t][2] epilogue start, [t][3] end
     uint64_t *trace;
@@ -122,13 +128,19 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     const size_t SB = (size_t)(KBt < TC_KBS ? KBt : TC_KBS) * TC_BOX;
     uint64_t *lists = (uint64_t *)(sX + (size_t)NS * SB);
     float *stage = (float *)(lists + (size_t)TC_BM * EPI * KP);
-    uint64_t *bars = (uint64_t *)(stage + 32 * TC_BM * EPI);
+    // row norms (and fp8 scales) of a tile, TC_NR tiles in flight: the
+    // producer copies them beside the tile's rows, the epilogue reads them
+    // as broadcasts (slot = [norms 128][scales 128])
+    float *snorm = stage + 32 * TC_BM * EPI;
+    uint64_t *bars = (uint64_t *)(snorm + (size_t)TC_NR * TC_NSLOT_F);
     uint64_t *full = bars;            // [NS]
     uint64_t *empty = full + NS;      // [NS]
     uint64_t *tfull = empty + NS;     // [2]
     uint64_t *tempty = tfull + 2;     // [2]
     uint64_t *qbar = tempty + 2;      // [1]
     uint64_t *done = qbar + 1;        // [1]
+    uint64_t *nfull = done + 1;       // [TC_NR]
+    uint64_t *nempty = nfull + TC_NR; // [TC_NR]
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
 
@@ -154,6 +166,10 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             mbar_init(&tfull[i], 1);
             mbar_init(&tempty[i], TC_BM * EPI);
         }
+        for (int i = 0; i < TC_NR; i++) {
+            mbar_init(&nfull[i], 1);
+            mbar_init(&nempty[i], 4 * EPI);  // one arrival per epilogue warp
+        }
         mbar_init(qbar, 1);
         mbar_init(done, 1);
         fence_mbar_init();
@@ -176,10 +192,27 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             for (int kb = 0; kb < KBt; kb++)
                 tma_load_2d(sQ + (size_t)kb * TC_BOX, &tmQ, kb * (FP8 ? 128 : 64),
                             qtile * TC_BM, qbar);
-            uint64_t it = 0;
+            const uint32_t nbytes = (FP8 ? 2 : 1) * TC_BN * 4;
+            uint64_t it = 0, nt = 0;  // stages and norm slots issued
             bool ok = true;
             for (uint64_t t = 0; t < ntiles && ok; t++) {
-                const int y = (int)((tile0 + t * a.tile_step) * TC_BN);
+                const uint64_t tile = tile0 + t * a.tile_step;
+                const int y = (int)(tile * TC_BN);
+                // the tile's norms (and scales): arrays are padded to whole
+                // tiles, rows of a tile are 512 contiguous bytes
+                {
+                    const int ns = (int)(t % TC_NR);
+                    if (!mbar_wait(&nempty[ns], (uint32_t)(((t / TC_NR) & 1) ^ 1), deadline,
+                                   abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&nfull[ns], nbytes);
+                    float *dst = snorm + (size_t)ns * TC_NSLOT_F;
+                    bulk_load(dst, a.xnorm + tile * TC_BN, TC_BN * 4, &nfull[ns]);
+                    if (FP8) bulk_load(dst + TC_BN, a.xscale + tile * TC_BN, TC_BN * 4, &nfull[ns]);
+                    nt = t + 1;
+                }
                 for (int kc = 0; kc < nkc; kc++, it++) {
                     const int s = (int)(it % NS);
                     const uint32_t ph = (uint32_t)((it / NS) & 1);
@@ -198,11 +231,14 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 atomicExch(a.err, 1);
             }
             // copies still in flight land before the CTA leaves
-            const uint64_t first = it > (uint64_t)NS ? it - NS : 0;
-            const uint64_t d2 = globaltimer() + a.timeout_ns;
+            const uint64_t d2 = globaltimer() + a.drain_ns;
             volatile int zero = 0;
+            const uint64_t first = it > (uint64_t)NS ? it - NS : 0;
             for (uint64_t j = first; j < it; j++)
                 mbar_wait(&full[j % NS], (uint32_t)((j / NS) & 1), d2, &zero);
+            const uint64_t nfirst = nt > (uint64_t)TC_NR ? nt - TC_NR : 0;
+            for (uint64_t j = nfirst; j < nt; j++)
+                mbar_wait(&nfull[j % TC_NR], (uint32_t)((j / TC_NR) & 1), d2, &zero);
             mbar_wait(qbar, 0, d2, &zero);
         }
     } else if (warp == 1) {
@@ -245,7 +281,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             // all issued MMAs complete before TMEM is released
             mma_commit(done);
             volatile int zero = 0;
-            mbar_wait(done, 0, globaltimer() + a.timeout_ns, &zero);
+            mbar_wait(done, 0, globaltimer() + a.drain_ns, &zero);
         }
     } else {
         // ------------------------------------------------ epilogue
@@ -277,19 +313,15 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         uint64_t thr = qvalid ? KEY_MAX : 0ull;  // admission threshold
         float thr_d = qvalid ? __int_as_float(0x7f800000) : -1.f;  // its distance
         bool ok = true;
-        // per-tile inputs, loaded one tile ahead: row norms (and fp8 scales),
-        // predicate words of the 32-row chunks, the grid-wide bound
-        float xr[CPH], xs[CPH];
-        uint32_t bw[CPH];
-        unsigned long long gt = KEY_MAX;
-        auto load_tile = [&](uint64_t tt, float (&x)[CPH], float (&s)[CPH], uint32_t (&w)[CPH],
-                             unsigned long long &g) {
+        // per-tile words in registers, loaded one tile ahead into the set the
+        // previous tile released (two sets, no register moves: a move would
+        // wait for the load): predicate words of the 32-row chunks and the
+        // grid-wide bound
+        auto load_words = [&](uint64_t tt, uint32_t (&w)[CPH], unsigned long long &g) {
             const uint64_t rb = (tile0 + tt * a.tile_step) * TC_BN + col0;
 #pragma unroll
             for (int j = 0; j < CPH; j++) {
                 if (j >= nch) break;
-                x[j] = __ldg(a.xnorm + rb + j * 32 + lane);
-                s[j] = FP8 ? __ldg(a.xscale + rb + j * 32 + lane) : 1.f;
                 const uint64_t r0 = rb + j * 32;
                 uint32_t v = 0;
                 if (r0 < a.nrows) {
@@ -300,24 +332,23 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             }
             g = qvalid ? *((volatile unsigned long long *)(a.tau + qg)) : KEY_MAX;
         };
-        // two tiles ahead: a tile's epilogue is shorter than a load's latency
-        float nxr[CPH], nxs[CPH];
-        uint32_t nbw[CPH];
-        unsigned long long ngt = KEY_MAX;
-        if (ntiles) load_tile(0, xr, xs, bw, gt);
-        if (ntiles > 1) load_tile(1, nxr, nxs, nbw, ngt);
-        for (uint64_t t = 0; t < ntiles; t++) {
+        // one tile: false when a wait gave up
+        auto tile_body = [&](uint64_t t, const uint32_t (&bw)[CPH], unsigned long long gt,
+                             uint32_t (&nbw)[CPH], unsigned long long &ngt) -> bool {
+            if (t + 1 < ntiles) load_words(t + 1, nbw, ngt);
             const int acc = (int)(t & 1);
             const uint32_t aph = (uint32_t)((t >> 1) & 1);
-            float n2xr[CPH], n2xs[CPH];
-            uint32_t n2bw[CPH];
-            unsigned long long n2gt = KEY_MAX;
-            if (t + 2 < ntiles) load_tile(t + 2, n2xr, n2xs, n2bw, n2gt);
-            if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) { ok = false; break; }
+            const int ns = (int)(t % TC_NR);
+            if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) return false;
+            if (!mbar_wait(&nfull[ns], (uint32_t)((t / TC_NR) & 1), deadline, abort_flag))
+                return false;
             tc_fence_after();
-            const bool tr = a.trace && blockIdx.x == 0 && slot == 0 && t < (uint64_t)a.trace_tiles;
+            const bool tr =
+                a.trace && blockIdx.x == 0 && slot == 0 && t < (uint64_t)a.trace_tiles;
             if (tr) a.trace[t * 4 + 2] = globaltimer();
             const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN + col0;
+            const float *xnv = snorm + (size_t)ns * TC_NSLOT_F + col0;
+            const float *xsv = xnv + TC_BN;
             if (gt < thr) {
                 thr = gt;
                 thr_d = key_dist(gt);
@@ -335,14 +366,22 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 // norm-form value is clamped there)
                 uint32_t cmask = 0;
 #pragma unroll
-                for (int i = 0; i < 32; i++) {
-                    const float xn = __shfl_sync(0xffffffffu, xr[c], i);
-                    float dot = __uint_as_float(r[i]);
-                    if (FP8) dot *= __shfl_sync(0xffffffffu, xs[c], i) * qs;
-                    const float d = fmaf(-2.f, dot, xn + qn);
-                    if (d <= thr_d) {
-                        stage[i * NSLOT + slot] = d;
-                        cmask |= 1u << i;
+                for (int i4 = 0; i4 < 32; i4 += 4) {
+                    const float4 xn4 = *(const float4 *)(xnv + c * 32 + i4);
+                    float4 xs4 = make_float4(1.f, 1.f, 1.f, 1.f);
+                    if (FP8) xs4 = *(const float4 *)(xsv + c * 32 + i4);
+                    const float xna[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
+                    const float xsa[4] = {xs4.x, xs4.y, xs4.z, xs4.w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int i = i4 + u;
+                        float dot = __uint_as_float(r[i]);
+                        if (FP8) dot *= xsa[u] * qs;
+                        const float d = fmaf(-2.f, dot, xna[u] + qn);
+                        if (d <= thr_d) {
+                            stage[i * NSLOT + slot] = d;
+                            cmask |= 1u << i;
+                        }
                     }
                 }
                 cmask &= bw[c];
@@ -397,19 +436,18 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
             }
             tc_fence_before();
             mbar_arrive(&tempty[acc]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&nempty[ns]);
             if (tr) a.trace[t * 4 + 3] = globaltimer();
             if (a.push_tau && qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
-#pragma unroll
-            for (int j = 0; j < CPH; j++) {
-                xr[j] = nxr[j];
-                xs[j] = nxs[j];
-                bw[j] = nbw[j];
-                nxr[j] = n2xr[j];
-                nxs[j] = n2xs[j];
-                nbw[j] = n2bw[j];
-            }
-            gt = ngt;
-            ngt = n2gt;
+            return true;
+        };
+        uint32_t wA[CPH], wB[CPH];
+        unsigned long long gA = KEY_MAX, gB = KEY_MAX;
+        if (ntiles) load_words(0, wA, gA);
+        for (uint64_t t = 0; t < ntiles; t += 2) {
+            if (!tile_body(t, wA, gA, wB, gB)) { ok = false; break; }
+            if (t + 1 < ntiles && !tile_body(t + 1, wB, gB, wA, gA)) { ok = false; break; }
         }
         if (!ok) {
             s_abort = 1;
@@ -438,10 +476,13 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                 }
                 PV_L(j) = v;
             }
-            // the list's best kwrite keys join its query's dense run (one
-            // atomic per list); a full list reports its last key, below
-            // which it cannot have dropped anything
-            const int nw = n < a.kwrite ? n : a.kwrite;
+            // the list's best kwrite keys at or below the grid-wide bound join
+            // its query's dense run (one atomic per list: keys above the bound
+            // cannot be in the answer); a full list reports its last key,
+            // below which it cannot have dropped anything
+            const unsigned long long bound = *((volatile unsigned long long *)(a.tau + qg));
+            int nw = n < a.kwrite ? n : a.kwrite;
+            while (nw > 0 && PV_L(nw - 1) > bound) nw--;
             if (nw > 0) {
                 const uint64_t b0 = atomicAdd(a.dcnt + qg, (uint32_t)nw);
                 uint64_t *dst = a.dense + (uint64_t)qg * a.dcap;
@@ -940,7 +981,7 @@ static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
     return 1024 + (size_t)kblocks * TC_BOX +
            (size_t)NS * (kblocks < TC_KBS ? kblocks : TC_KBS) * TC_BOX +
            (size_t)TC_BM * EPI * KP * 8 + (size_t)32 * TC_BM * EPI * 4 +
-           (size_t)(2 * NS + 6) * 8;
+           (size_t)TC_NR * TC_NSLOT_F * 4 + (size_t)(2 * NS + 6 + 2 * TC_NR) * 8;
 }
 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
@@ -1104,7 +1145,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.kwrite = KP;
     a.fullmin = certify ? d_fullmin : nullptr;
     a.err = d_err;
-    a.timeout_ns = 2000000000ull;
+    a.timeout_ns = g->tc_timeout_ns ? g->tc_timeout_ns : 2000000000ull;
+    a.drain_ns = 2000000000ull;
     a.trace = nullptr;
     a.trace_tiles = 0;
     static const bool tracing = getenv("PV_TC_TRACE") != nullptr;
@@ -1141,10 +1183,10 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         // only each list's best keys: the S-th key of a subset of the
         // sample still bounds the S-th key of the scan, and a short run
         // keeps the merge cheap (the radix select of S > 32 reads its run
-        // 8 times; the S-th best of the sample rarely needs more than a
-        // few keys of any one list)
-        const int seed_keys = S <= 32 ? 8192 : 4096;
-        sa.kwrite = std::max(1, std::min(KP, seed_keys / std::max(1, nlists)));
+        // 8 times). The sample's S best keys are spread over many lists
+        // (S / nlists per list on average), so a list rarely holds more
+        // than two of them: 4S keys in all, at least two per list.
+        sa.kwrite = std::max(2, std::min(KP, (4 * S + nlists - 1) / std::max(1, nlists)));
         // lists need hold no more than that (short heaps admit fewer rows);
         // a full list's last key bounds the S-th key only if it holds S
         sa.KP = sa.kwrite;
@@ -1166,15 +1208,27 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
     uint8_t *d_unc = certify ? (uint8_t *)(c + off_unc) : nullptr;
-    PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, false, a.fullmin, a.tau, S, d_qprog,
-                                  popcnt, g->count, nq, cand, ccnt, (uint8_t *)(c + off_ctr),
-                                  nullptr, d_unc, g->stream),
-               errbuf, errlen);
+    if (S == (int)topb) {
+        // certified exact (integer rows and queries, all sums below 2^24):
+        // every norm-form distance already is the exact squared L2 distance,
+        // so the merged top-k is the answer and needs no re-rank
+        g->launches--;
+        PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, false, a.fullmin, a.tau, S,
+                                      d_qprog, popcnt, g->count, nq, d_out, d_cnt, d_trunc,
+                                      nullptr, d_unc, g->stream),
+                   errbuf, errlen);
+    } else {
+        PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, false, a.fullmin, a.tau, S,
+                                      d_qprog, popcnt, g->count, nq, cand, ccnt,
+                                      (uint8_t *)(c + off_ctr), nullptr, d_unc, g->stream),
+                   errbuf, errlen);
+        rerank_kernel<<<nq, 256, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, S, topb,
+                                                 d_qprog, popcnt, g->count, d_out, d_cnt,
+                                                 d_trunc);
+        PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    }
     g->tc_unc = d_unc;
     g->tc_unc_n = nq;
-    rerank_kernel<<<nq, 256, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, S, topb,
-                                             d_qprog, popcnt, g->count, d_out, d_cnt, d_trunc);
-    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
     if (ev) cudaEventRecord(ev[3], g->stream);
     g->tc_err = d_err;
     if (tracing && d_trace) {
