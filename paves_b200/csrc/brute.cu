@@ -136,9 +136,13 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         return 0;
     }
     if (mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0) {
+        // a staged batch with its counts on the device (the stream's graphs)
+        // may mark itself lazy: then it has no bitmaps (see stream.cu)
+        TcLazy lz{(const int *)(d + db.off_counts) + 3, d_progs, d_insns, d_consts,
+                  db.nconsts};
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
-                           errbuf, errlen))
+                           errbuf, errlen, db.counts_on_device ? &lz : nullptr))
             return -1;
         if (ev) cudaEventRecord(ev[4], g->stream);
         return 0;

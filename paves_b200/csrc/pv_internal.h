@@ -138,12 +138,23 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns);
 int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax);
 bool tc_supported(const FvGpuIndex *g);
+// Lazy filters for the tensor-core scan: *flag (device memory, read when
+// the kernel runs) != 0 means the batch has no bitmaps and every program is
+// in range form; the scan then evaluates a query's program only for rows
+// whose key beats its threshold (truncation flags are not computed).
+struct TcLazy {
+    const int *flag;
+    const PredProg *progs;
+    const PredInsn *insns;
+    const double *consts;
+    int nconsts;
+};
 int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen);
+                   size_t errlen, const TcLazy *lz = nullptr);
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);

@@ -88,6 +88,16 @@ struct TcArgs {
     const int32_t *__restrict__ qprog;
     const uint32_t *__restrict__ bitmaps;
     uint64_t bm_words;
+    // lazy filters: when *lazy != 0 the batch has no bitmaps; every program
+    // is in range form and is evaluated from the attribute columns only for
+    // rows whose key already beats the threshold (null: bitmaps)
+    const int *lazy;
+    const PredProg *__restrict__ progs;
+    const PredInsn *__restrict__ insns;
+    const double *__restrict__ consts;
+    int nconsts;
+    const double *__restrict__ cols;
+    int ncols;
     unsigned long long *tau;  // [nq] grid-wide bound
     // kept keys: each list appends its best kwrite keys to its query's dense
     // run dense[q][0 .. dcnt[q]) (any order; dcap >= lists per query * kwrite)
@@ -303,7 +313,58 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         const float qn = qvalid ? a.qnorm[qg] : 0.f;
         const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
         const int pg = qvalid ? a.qprog[qg] : -1;
-        const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
+        const bool lazy = a.lazy && *a.lazy;
+        const uint32_t *bm = (pg >= 0 && !lazy) ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
+        // lazy: the query's range program (AND of per-column intervals and
+        // small-integer sets, the encoding of common.cuh) in registers
+        int nterm = 0;
+        int tcol[PV_RANGE_MAX_TERMS];
+        double tlo[PV_RANGE_MAX_TERMS], thi[PV_RANGE_MAX_TERMS];
+        if (lazy && pg >= 0) {
+            const PredProg pp = a.progs[pg];
+            const PredInsn r = a.insns[pp.insn0];
+            int ci = r.val0;
+            nterm = min(max(r.n, 0), PV_RANGE_MAX_TERMS);
+#pragma unroll
+            for (int k = 0; k < PV_RANGE_MAX_TERMS; k++) {
+                tcol[k] = -1;  // a malformed term admits nothing
+                tlo[k] = 1.0;
+                thi[k] = 0.0;
+                if (k >= nterm || ci < 0 || ci + 2 > a.nconsts) continue;
+                const int meta = (int)a.consts[ci];
+                const int col = meta & 0xFFFF;
+                const bool mask = meta & PV_TERM_MASK;
+                if (col < a.ncols && (mask || ci + 3 <= a.nconsts)) {
+                    tcol[k] = col | (mask ? PV_TERM_MASK : 0);
+                    tlo[k] = a.consts[ci + 1];  // a mask term: its bits
+                    thi[k] = mask ? 0.0 : a.consts[ci + 2];
+                }
+                ci += mask ? 2 : 3;
+            }
+        }
+        // the range program on row `row`: f64 compares, NaN fails (the
+        // bitmap kernel's test of the same encoding)
+        auto lazy_pass = [&](uint64_t row) -> bool {
+            bool ok = true;
+#pragma unroll
+            for (int k = 0; k < PV_RANGE_MAX_TERMS; k++) {
+                if (k >= nterm) break;
+                if (tcol[k] < 0) return false;
+                const int col = tcol[k] & 0xFFFF;
+                const double v = __ldg(a.cols + (uint64_t)col * a.nrows + row);
+                if (tcol[k] & PV_TERM_MASK) {
+                    const bool in = v >= 0.0 && v < 64.0;
+                    const int b = in ? (int)v : 64;
+                    const int code = (in && (double)b == v) ? b : 64;
+                    const unsigned long long bits =
+                        (unsigned long long)__double_as_longlong(tlo[k]);
+                    ok = ok && code < 64 && ((bits >> (code & 63)) & 1ull);
+                } else {
+                    ok = ok && v >= tlo[k] && v <= thi[k];
+                }
+            }
+            return ok;
+        };
         // thread-private list, interleaved [KP][NSLOT] so a warp's accesses to
         // the same slot index hit 32 different banks
         uint64_t *L = lists + slot;
@@ -395,6 +456,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
                     // <= : the seeded bound is itself a row key that this
                     // pass must admit again (keys are unique)
                     if (key > thr) continue;
+                    if (lazy && !lazy_pass(row)) continue;
                     // the list is a max-heap (root = worst kept key): an
                     // admission costs O(log KP) shared-memory steps
                     if (n < KP) {
@@ -1015,7 +1077,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen) {
+                   size_t errlen, const TcLazy *lz) {
     const bool fp8 = g->precision == FV_GPU_PREC_FP8;
     const int esz = fp8 ? 1 : 2;
     const int kblocks = g->kpad * esz / TC_KB_BYTES;
@@ -1138,6 +1200,13 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.qprog = d_qprog;
     a.bitmaps = bitmaps;
     a.bm_words = bm_words;
+    a.lazy = lz ? lz->flag : nullptr;
+    a.progs = lz ? lz->progs : nullptr;
+    a.insns = lz ? lz->insns : nullptr;
+    a.consts = lz ? lz->consts : nullptr;
+    a.nconsts = lz ? lz->nconsts : 0;
+    a.cols = g->d_cols;
+    a.ncols = g->ncols;
     a.tau = s.tau.as<unsigned long long>();
     a.dense = s.part.as<uint64_t>();
     a.dcnt = d_dcnt;

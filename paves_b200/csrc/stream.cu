@@ -130,10 +130,19 @@ int stage(Bucket &b, const FvGpuIndex *g, int nq, const float *queries, const Pr
         memcpy(h + b.db.off_insns, pb.insns.data(), pb.insns.size() * sizeof(PredInsn));
     if (!pb.consts.empty())
         memcpy(h + b.db.off_consts, pb.consts.data(), pb.consts.size() * 8);
+    // lazy filters (tensor-core buckets whose programs are all in range
+    // form): no bitmaps, the scan tests a query's filter only on rows that
+    // beat its threshold, instead of one full bitmap per query
+    bool lazy = b.mode == PV_MODE_LOW;
+    for (int p = 0; p < P && lazy; p++) {
+        const PredProg &pp = pb.progs[p];
+        lazy = pp.ninsn == 1 && pb.insns[pp.insn0].kind == PV_NODE_RANGE;
+    }
     int32_t *cnt = (int32_t *)(h + b.db.off_counts);
-    cnt[0] = P;
+    cnt[0] = lazy ? 0 : P;
     cnt[1] = (int)pb.insns.size();
     cnt[2] = (int)pb.consts.size();
+    cnt[3] = lazy ? 1 : 0;
     return 0;
 }
 

@@ -95,3 +95,27 @@ def test_predicate_overflow_takes_the_ordinary_path(env):
     ids, dists, cnt, ms = s.run(q, [big], 10)
     assert s.last()["fallback"] == 1
     assert _check(ds, q, [big], np.array([10]), ids, dists, cnt) >= 0.99
+
+
+def test_lazy_and_bitmap_filters_in_one_stream(env):
+    """Batches whose filters are all ranges / small-integer sets are tested
+    lazily inside the scan (no bitmaps); a batch with an OR or NOT filter
+    takes the bitmaps. Both must give the oracle's answers, also when they
+    alternate on the same captured graph."""
+    ds, g, s, path = env
+    rng = np.random.default_rng(11)
+    P, Cc = datagen.COL_PRICE, datagen.COL_CATEGORY
+    orf = pred.Or(pred.Cmp(P, "<", 30.0), pred.In(Cc, [2.0]))
+    notf = pred.Not(pred.Cmp(P, "<", 900.0))
+    for rep in range(3):
+        for mix in ("lazy", "bitmap"):
+            nq = 16
+            q = ds.queries[rng.choice(256, nq, replace=False)]
+            preds = [random_filter(rng) for _ in range(nq)]
+            if mix == "bitmap":
+                preds[3] = orf
+                preds[9] = notf
+            k = rng.choice(np.array([1, 10, 100], np.uint32), nq)
+            ids, dists, cnt, ms = s.run(q, preds, k)
+            assert s.last()["fallback"] == 0
+            assert _check(ds, q, preds, k, ids, dists, cnt) >= 0.98, (rep, mix)
