@@ -94,6 +94,21 @@ int pv_hnsw_info(const PvHnsw *h, uint32_t *M, int *max_level, uint64_t *entry,
  * [count+1], upper [upper_len] (any pointer may be NULL). */
 int pv_hnsw_export(const PvHnsw *h, uint32_t *l0, uint8_t *levels, uint64_t *upper_offs,
                    uint32_t *upper);
+/* The same sections built on the GPU (no counterpart in the reference,
+ * whose builder is CPU-only, engine_api.h:45 fv_builder_finish): every
+ * level from exact nearest neighbours instead of insertion-time beam
+ * searches. Per level, each node's `candidates` nearest nodes of that level
+ * (this library's exact scans, the nodes as queries; BF16 tensor cores when
+ * certified exact, precision FV_GPU_PREC_BF16, else FP32), the
+ * neighbour-selection rule (keep a candidate closer to the node than to
+ * every kept neighbour) to 2M at level 0 / M above, reverse edges, and the
+ * rule again over forward + reverse candidates. Node levels are drawn as
+ * the host builder draws them; the entry node is the lowest-numbered node
+ * of the top level. The graph differs from the host builder's; it is
+ * searched by the same code. candidates in [2M, 1023]; NULL + errbuf on
+ * bad parameters or a device error. */
+PvHnsw *pv_hnsw_build_gpu(const float *vectors, uint64_t count, int dim, int M, int candidates,
+                          int device, int precision, char *errbuf, size_t errlen);
 /* Level-0 entry point per query by greedy descent through the upper levels
  * (engine_api.h:199 fv_index_graph_entry), parallel over queries. */
 int pv_hnsw_entries(const float *vectors, int dim, const uint64_t *upper_offs,

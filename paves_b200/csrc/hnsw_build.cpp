@@ -299,6 +299,48 @@ extern "C" PvHnsw *pv_hnsw_build(const float *vectors, uint64_t count, int dim, 
     return h;
 }
 
+namespace pv {
+
+// Sections of a graph over count rows (levels drawn as above, zeroed lists)
+// for builders that fill the lists themselves (the GPU builder).
+PvHnsw *hnsw_sections(const float *vectors, uint64_t count, int dim, int M) {
+    PvHnsw *h = new PvHnsw();
+    h->vec = vectors;
+    h->dim = dim;
+    h->n = count;
+    h->M = (uint32_t)M;
+    h->M0 = 2 * (uint32_t)M;
+    h->efc = 0;
+    h->level.resize(count);
+    const double mult = 1.0 / log((double)M);
+    h->upper_off.resize(count + 1);
+    uint64_t slots = 0;
+    for (uint64_t i = 0; i < count; i++) {
+        double u = (double)(mix64(i * 0x5851F42D4C957F2DULL + 12345) >> 11) *
+                   (1.0 / 9007199254740992.0);
+        if (u < 1e-18) u = 1e-18;
+        int lv = (int)(-log(u) * mult);
+        if (lv > 30) lv = 30;
+        h->level[i] = (uint8_t)lv;
+        h->upper_off[i] = slots;
+        slots += (uint64_t)lv * (M + 1);
+    }
+    h->upper_off[count] = slots;
+    h->upper.assign(slots, 0);
+    h->l0.assign(count * (uint64_t)(h->M0 + 1), 0);
+    return h;
+}
+const uint8_t *hnsw_levels(const PvHnsw *h) { return h->level.data(); }
+uint32_t *hnsw_l0(PvHnsw *h) { return h->l0.data(); }
+uint32_t *hnsw_upper_list(PvHnsw *h, uint64_t node, int level) { return h->list(node, level); }
+void hnsw_set_entry(PvHnsw *h, uint64_t entry, int level, int efc) {
+    h->entry.store(entry);
+    h->entry_level.store(level);
+    h->efc = (uint32_t)efc;
+}
+
+}  // namespace pv
+
 extern "C" void pv_hnsw_free(PvHnsw *h) { delete h; }
 
 extern "C" int pv_hnsw_info(const PvHnsw *h, uint32_t *M, int *max_level, uint64_t *entry,

@@ -159,6 +159,16 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);
 
+// ---- HNSW sections (hnsw_build.cpp) for the GPU builder (hnsw_gpu.cu)
+}  // namespace pv
+typedef struct PvHnsw PvHnsw;
+namespace pv {
+PvHnsw *hnsw_sections(const float *vectors, uint64_t count, int dim, int M);
+const uint8_t *hnsw_levels(const PvHnsw *h);
+uint32_t *hnsw_l0(PvHnsw *h);
+uint32_t *hnsw_upper_list(PvHnsw *h, uint64_t node, int level);
+void hnsw_set_entry(PvHnsw *h, uint64_t entry, int level, int efc);
+
 // ---- graph search (graph.cu)
 // ---- graph search (graph.cu)
 struct GraphOut {

@@ -18,15 +18,33 @@ from ._lib import ptr
 
 
 class Hnsw:
+    """builder "host": the multi-threaded insertion builder (the engine's
+    construction, pv_hnsw_build); "gpu": the bulk GPU builder
+    (pv_hnsw_build_gpu) from each node's `candidates` exact nearest
+    neighbours (default 4M - 1), on `device`, with BF16 tensor-core scans
+    when the rows are integers the BF16 path computes exactly, else FP32."""
+
     def __init__(self, vectors: np.ndarray, M: int = 16, ef_construction: int = 200,
-                 threads: int = 0):
+                 threads: int = 0, builder: str = "host", device: int = 0,
+                 candidates: int = 0):
         L = _lib.lib()
         self.vectors = np.ascontiguousarray(vectors, np.float32)
         n, d = self.vectors.shape
         err = C.create_string_buffer(256)
-        h = L.pv_hnsw_build(ptr(self.vectors), n, d, M, ef_construction, threads, err, 256)
+        if builder == "gpu":
+            v = self.vectors
+            integral = bool(np.all(np.abs(v) <= 256.0) and np.array_equal(v, np.rint(v)))
+            prec = _lib.FV_GPU_PREC_BF16 if integral else _lib.FV_GPU_PREC_FP32
+            cand = candidates or min(1023, 4 * M - 1)
+            h = L.pv_hnsw_build_gpu(ptr(v), n, d, M, cand, device, prec, err, 256)
+            ef_construction = cand
+        elif builder == "host":
+            h = L.pv_hnsw_build(ptr(self.vectors), n, d, M, ef_construction, threads, err, 256)
+        else:
+            raise ValueError(f"unknown builder {builder!r}")
         if not h:
             raise RuntimeError(err.value.decode())
+        self.builder = builder
         try:
             m = C.c_uint32()
             lvl = C.c_int()
@@ -72,12 +90,12 @@ class Hnsw:
 
 
 def build_or_load(vectors: np.ndarray, cache: Optional[str], M: int = 16,
-                  ef_construction: int = 200) -> Hnsw:
+                  ef_construction: int = 200, builder: str = "host", device: int = 0) -> Hnsw:
     """Builds a graph, or reloads the sections saved at `cache` (npz) when
     they were built from identical rows and parameters."""
     import hashlib
     key = hashlib.sha256(np.ascontiguousarray(vectors[:: max(1, len(vectors) // 4096)])
-                         .tobytes()).hexdigest()[:16] + f"_{len(vectors)}_{M}_{ef_construction}"
+                         .tobytes()).hexdigest()[:16] + f"_{len(vectors)}_{M}_{ef_construction}_{builder}"
     if cache and os.path.exists(cache):
         z = np.load(cache)
         if str(z["key"]) == key:
@@ -87,8 +105,9 @@ def build_or_load(vectors: np.ndarray, cache: Optional[str], M: int = 16,
             h.l0, h.levels = z["l0"], z["levels"]
             h.upper_offs, h.upper = z["upper_offs"], z["upper"]
             h.ef_construction = ef_construction
+            h.builder = builder
             return h
-    h = Hnsw(vectors, M, ef_construction)
+    h = Hnsw(vectors, M, ef_construction, builder=builder, device=device)
     if cache:
         tmp = f"{cache}.{os.getpid()}.tmp.npz"
         np.savez(tmp, key=key, M=h.M, max_level=h.max_level, entry=h.entry_node, l0=h.l0,
