@@ -431,7 +431,9 @@ def graph_bench(args):
     from concurrent.futures import ThreadPoolExecutor
     ds, _, _ = make_workload()
     cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
+    t0 = time.perf_counter()
     h = shared_graph(ds.vectors, 0, None, cache)
+    build_s = time.perf_counter() - t0
     gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
     L = _lib.lib()
     q = ds.queries[:BATCH]
@@ -460,6 +462,34 @@ def graph_bench(args):
                         "qps_e2e": round(BATCH * reps / wall, 1),
                         "mean_steps": round(float(st[:, 0].mean()), 1),
                         "mean_visited": round(float(st[:, 1].mean()), 1)})
+    # the same searches on the graph the GPU builder makes (pv_hnsw_build_gpu)
+    gpu_built = {}
+    try:
+        from paves_b200.hnsw import Hnsw
+        t0 = time.perf_counter()
+        hg = Hnsw(ds.vectors, 16, builder="gpu")
+        gpu_built["build_s"] = round(time.perf_counter() - t0, 2)
+        gg = GpuIndex(ds.vectors, ds.cols, l0=hg.l0)
+        entg = hg.entries(q)
+        rows = []
+        for name, p in datagen.graph_predicates().items():
+            preds = [p] * BATCH
+            xi, _, xc, _ = gi.brute_batch(q, preds, TOPK)
+            for ef in (32, 64, 128, 256):
+                gg.graph_batch(q, entg, preds, ef)
+                dev = 0.0
+                reps = max(1, min(args.steps, 10))
+                for _ in range(reps):
+                    ids, _, cnt, _ = gg.graph_batch(q, entg, preds, ef)
+                    dev += L.pv_last_kernel_ms(gg.handle)
+                rec = float(np.mean([np.isin(xi[i, :xc[i]], ids[i, :TOPK]).sum() /
+                                     max(1, int(xc[i])) for i in range(BATCH)]))
+                rows.append({"filter": name, "ef": ef, "recall_at_10": round(rec, 4),
+                             "qps": round(BATCH * reps / (dev / 1e3), 1)})
+        gpu_built["results"] = rows
+        gg.close()
+    except Exception as e:  # informative
+        gpu_built = {"failed": str(e)}
     ref = []
     try:
         from oracle import refengine
@@ -528,7 +558,8 @@ def graph_bench(args):
             "config": {"workload": "1M x 128 Gaussian-mixture rows, HNSW M=16 efC=200 built by "
                                    "the library, 64-query batches, filters 1%/10%/50%, top-10",
                        "rows": N_ROWS, "dim": DIM, "batch": BATCH, "k": TOPK},
-            "results": res, "reference_cpu": ref, "reference_gpu": ref_gpu}
+            "host_build_s": round(build_s, 1), "results": res, "gpu_built_graph": gpu_built,
+            "reference_cpu": ref, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
     gi.close()
 
