@@ -829,7 +829,7 @@ def main():
 
     barrier()
     clk = Clocks(local)
-    dev_ms, launches, graph_steps = 0.0, 0, 0
+    dev_ms, launches, graph_steps, mixed_steps = 0.0, 0, 0, 0
     st_sum = np.zeros(3)
     results = {}
     t0 = time.perf_counter()
@@ -839,7 +839,8 @@ def main():
         dev_ms += float(st[0] + st[2])  # routing runs beside the search
         st_sum += st
         launches += int(L.pv_last_launches(gi.handle))
-        graph_steps += ex
+        graph_steps += int(ex == 1)
+        mixed_steps += int(ex == 2)
         results[c] = (ids, cnt, dec, ex, dists)
     wall_s = time.perf_counter() - t0
     clocks = clk.stop()
@@ -857,7 +858,7 @@ def main():
         r = [np.isin(xi[i, :xc[i]], ids[i, :cnt[i]]).sum() / max(1, int(xc[i]))
              for i in range(BATCH)]
         recall[name] = {"recall_at_10": round(float(np.mean(r)), 4),
-                        "path": "graph" if ex else "bf16-scan",
+                        "path": {0: "bf16-scan", 1: "graph", 2: "mixed"}[int(ex)],
                         "graph_queries": int((dec > 0).sum())}
 
     # the scan path without the router (each class batch, prepared); the
@@ -941,6 +942,7 @@ def main():
             "recall_per_class": recall,
             "recall_at_10_min": round(min(v["recall_at_10"] for v in recall.values()), 4),
             "graph_batches": graph_steps,
+            "mixed_batches": mixed_steps,
             "routed_stage_ms": {"bitmaps": round(st_sum[0] / args.steps, 4),
                                 "routing_beside_search": round(st_sum[1] / args.steps, 4),
                                 "search": round(st_sum[2] / args.steps, 4)},

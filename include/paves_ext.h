@@ -252,20 +252,21 @@ int pv_router_train(PvRouter *r, int n, const float *feats, const int32_t *label
 
 /* Learned-routed filtered top-k batch (no reference counterpart): builds
  * the batch's predicate bitmaps, computes the router's features and MLP
- * action per query on the device, then answers the whole batch by the
- * graph search (per-query ef) when every query was routed to the graph,
- * else by the scan of the index's precision (a scan costs about the same
- * for one query as for a query tile, and its results are exact, so a batch
- * with any scan-routed query scans). The scan starts speculatively beside
- * the routing and is discarded when the batch goes to the graph. plan (optional, replaces the router,
- * r may then be NULL): per query 0 = scan or the beam width to use. k[nq]
- * <= topb; out has stride topb and holds min(k, found) hits per query.
- * qd[i].entry must hold the level-0 entry point when the index has a
- * graph. decided[nq] (optional) receives each query's beam width (0 =
- * scan), *executed 1 for the graph, 0 for the scan; stage_ms[3] the device
- * time of the bitmaps, of the routing (features, MLP, decision read back;
- * it runs on a second stream beside a speculative scan) and of the search
- * after the bitmaps: the batch took stage_ms[0] + stage_ms[2]. */
+ * action per query on the device, and answers each query by the route
+ * chosen for it: the graph search at its beam width, or the scan of the
+ * index's precision. The scan starts speculatively beside the routing (a
+ * scan costs about the same for one query as for a query tile); the graph
+ * search runs, on a second stream, for the graph-routed queries only, and
+ * a batch whose every query went to the graph discards the scan. plan
+ * (optional, replaces the router, r may then be NULL): per query 0 = scan
+ * or the beam width to use. k[nq] <= topb; out has stride topb and holds
+ * min(k, found) hits per query. qd[i].entry must hold the level-0 entry
+ * point when the index has a graph. decided[nq] (optional) receives each
+ * query's beam width (0 = scan), *executed 0 when every query was scanned,
+ * 1 when every query took the graph, 2 for a mixed batch; stage_ms[3] the
+ * device time of the bitmaps, of the routing (features, MLP, decision read
+ * back; it runs beside the speculative scan) and of the search after the
+ * bitmaps: the batch took stage_ms[0] + stage_ms[2]. */
 int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *queries,
                     const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,

@@ -144,8 +144,19 @@ __global__ void __launch_bounds__(G_THREADS) graph_kernel(GraphArgs a) {
 
     const int q = blockIdx.x;
     const int tid = threadIdx.x;
+    // a per-query beam width of 0: the query is answered elsewhere (a mixed
+    // routed batch scans it), nothing to search
+    if (a.efq && a.efq[q] == 0) {
+        if (tid == 0) {
+            a.out_cnt[q] = 0;
+            a.out_exh[q] = 0;
+            if (a.stats)
+                for (int i = 0; i < 4; i++) a.stats[q * 4 + i] = 0;
+        }
+        return;
+    }
     // per-query beam width (never above the batch's, which is the output stride)
-    const int ef = a.efq ? max(1, min((int)a.efq[q], a.ef)) : a.ef;
+    const int ef = a.efq ? min((int)a.efq[q], a.ef) : a.ef;
     const int pg = a.qprog[q];
     const uint32_t *bm = pg >= 0 ? a.bitmaps + (uint64_t)pg * a.bm_words : nullptr;
     uint32_t *vb = a.visited_bits + (uint64_t)q * a.bm_words;

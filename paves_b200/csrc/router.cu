@@ -976,68 +976,86 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
         RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
     }
     RT_OK(cudaEventSynchronize(ev[2]));
-    bool all_graph = have_graph;
+    // each query takes the route the router chose for it: the graph search
+    // at its beam width (graph-routed queries, when the index has a graph)
+    // or the scan; a batch whose every query went to the graph discards
+    // the speculative scan
+    int ngraph = 0;
     uint32_t efmax = 0;
     for (int i = 0; i < nq; i++) {
-        if (hefq[i] == 0) all_graph = false;
+        if (!have_graph) hefq[i] = 0;
+        if (hefq[i] > 0) ngraph++;
         efmax = hefq[i] > efmax ? hefq[i] : efmax;
     }
+    const bool all_graph = have_graph && ngraph == nq;
     if (decided) memcpy(decided, hefq, (size_t)nq * 2);
-    if (executed) *executed = all_graph ? 1 : 0;
+    if (executed) *executed = ngraph == 0 ? 0 : all_graph ? 1 : 2;
+    if (!spec && !all_graph) {  // a plan sent every query to a graph the index lacks
+        if (errbuf && errlen) snprintf(errbuf, errlen, "routed: no graph for the plan");
+        return -1;
+    }
     cudaEvent_t done = ev[3];
-    if (all_graph) {
-        const GraphOut lo = graph_out_layout(nq, efmax);
+    const char *goh = nullptr;
+    GraphOut glo{};
+    if (ngraph > 0) {
+        glo = graph_out_layout(nq, efmax);
         char *oh = g->graph.route_h.as<char>() + eb;
         char *od = g->graph.gout.as<char>();
         const uint64_t mv = (uint64_t)efmax * 400 > 200000 ? (uint64_t)efmax * 400 : 200000;
         if (graph_launch(g, nq, (const float *)(d + db.off_q), (const uint32_t *)(dx + 2 * n4),
-                         (const int32_t *)(d + db.off_qprog), defq, efmax, mv, od, lo, errbuf,
+                         (const int32_t *)(d + db.off_qprog), defq, efmax, mv, od, glo, errbuf,
                          errlen, side))
             return -1;
         RT_OK(cudaEventRecord(ev[4], side));
-        RT_OK(cudaMemcpyAsync(oh, od, lo.bytes, cudaMemcpyDeviceToHost, side));
+        RT_OK(cudaMemcpyAsync(oh, od, glo.bytes, cudaMemcpyDeviceToHost, side));
         RT_OK(cudaStreamSynchronize(side));
-        RT_OK(cudaStreamSynchronize(g->stream));  // the speculative scan, if any
-        if (spec && check_tc_watchdog(g, errbuf, errlen)) return -1;
-        g->tc_unc = nullptr;
-        const uint32_t *cnt = (const uint32_t *)(oh + lo.off_cnt);
-        for (int q = 0; q < nq; q++) {
-            uint32_t c = cnt[q] < k[q] ? cnt[q] : k[q];
-            memcpy(out + (size_t)q * topb, oh + (size_t)q * efmax * sizeof(FvHit),
+        goh = oh;
+        g->graph_stats.resize((size_t)nq * 4);
+        memcpy(g->graph_stats.data(), oh + glo.off_st, (size_t)nq * 16);
+    }
+    RT_OK(cudaStreamSynchronize(g->stream));  // the scan, if any
+    if (spec && check_tc_watchdog(g, errbuf, errlen)) return -1;
+    const char *soh = s.out_h.as<char>();
+    const uint32_t *scnt = (const uint32_t *)(soh + off_cnt);
+    const uint32_t *gcnt = goh ? (const uint32_t *)(goh + glo.off_cnt) : nullptr;
+    for (int q = 0; q < nq; q++) {
+        if (hefq[q] > 0) {
+            const uint32_t c = gcnt[q] < k[q] ? gcnt[q] : k[q];
+            memcpy(out + (size_t)q * topb, goh + (size_t)q * efmax * sizeof(FvHit),
+                   c * sizeof(FvHit));
+            out_cnt[q] = c;
+        } else {
+            const uint32_t c = scnt[q] < k[q] ? scnt[q] : k[q];
+            memcpy(out + (size_t)q * topb, soh + (size_t)q * topb * sizeof(FvHit),
                    c * sizeof(FvHit));
             out_cnt[q] = c;
         }
-        g->graph_stats.resize((size_t)nq * 4);
-        memcpy(g->graph_stats.data(), oh + lo.off_st, (size_t)nq * 16);
-        done = ev[4];
-    } else {
-        if (!spec) {  // a plan sent every query to a graph the index lacks
-            if (errbuf && errlen) snprintf(errbuf, errlen, "routed: no graph for the plan");
-            return -1;
-        }
+    }
+    if (spec && g->tc_unc && ngraph < nq) {
+        // scan-routed queries whose reduced-precision superset the merge
+        // could not certify are re-run exactly
+        std::vector<uint8_t> unc(nq), tr(nq);
+        RT_OK(cudaMemcpyAsync(unc.data(), g->tc_unc, (size_t)nq, cudaMemcpyDeviceToHost,
+                              g->stream));
         RT_OK(cudaStreamSynchronize(g->stream));
-        if (check_tc_watchdog(g, errbuf, errlen)) return -1;
-        const char *oh = s.out_h.as<char>();
-        const uint32_t *cnt = (const uint32_t *)(oh + off_cnt);
-        for (int q = 0; q < nq; q++) {
-            uint32_t c = cnt[q] < k[q] ? cnt[q] : k[q];
-            memcpy(out + (size_t)q * topb, oh + (size_t)q * topb * sizeof(FvHit), c * sizeof(FvHit));
-            out_cnt[q] = c;
-        }
-        std::vector<uint8_t> tr(nq);
-        if (tc_redo_uncertain(g, nq, queries, pb, topb, out, out_cnt, tr.data(), errbuf, errlen))
+        for (int q = 0; q < nq; q++)
+            if (hefq[q] > 0) unc[q] = 0;
+        if (redo_flagged(g, nq, queries, pb, topb, unc.data(), out, out_cnt, tr.data(), errbuf,
+                         errlen))
             return -1;
         for (int q = 0; q < nq; q++)
             if (out_cnt[q] > k[q]) out_cnt[q] = k[q];
     }
+    g->tc_unc = nullptr;
+    if (ngraph > 0) done = ev[4];
     // device time of the batch: bitmaps, then the search with the routing
     // beside it (t[1] overlaps t[2]; the batch took t[0] + t[2])
     float t[3] = {0, 0, 0}, tot = 0.f;
     cudaEventElapsedTime(&t[0], ev[0], ev[1]);
     cudaEventElapsedTime(&t[1], ev[1], ev[2]);
     cudaEventElapsedTime(&tot, ev[0], done);
-    if (all_graph && spec) {
-        float a = 0.f;  // the discarded scan may finish last
+    if (ngraph > 0 && spec) {
+        float a = 0.f;  // the scan may finish last
         cudaEventElapsedTime(&a, ev[0], ev[3]);
         if (a > tot) tot = a;
     }

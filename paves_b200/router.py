@@ -292,7 +292,7 @@ def routed_batch(index, router: Optional[Router], queries: np.ndarray, preds, k,
                  topb: Optional[int] = None, plan: Optional[np.ndarray] = None,
                  margin: float = 0.0, bp: Optional[BatchPred] = None):
     """pv_routed_batch -> (ids u64 [nq][topb], dists, cnt, decided ef per query,
-    executed (1 graph / 0 scan), stage_ms [3]: bitmaps, routing (beside the
+    executed (0 all scanned / 1 all graph / 2 mixed), stage_ms [3]: bitmaps, routing (beside the
     search), search; the batch took stage_ms[0] + stage_ms[2]). bp: the
     batch's predicate arrays with entries, if already built."""
     from .pred import concat

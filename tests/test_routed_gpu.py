@@ -68,10 +68,18 @@ def test_mixed_plan_scans_and_router_decisions(env):
     k = np.full(NQ, 10, np.uint32)
     plan = np.full(NQ, 64, np.uint16)
     plan[5] = 0
+    plan[11] = 0
     ids, dist, cnt, dec, ex, st = routed_batch(g, None, ds.queries, preds, k, ent, plan=plan)
-    assert ex == 0
+    assert ex == 2  # mixed: each query takes its own route
     bi, bd, bc, _ = g.brute_batch(ds.queries, preds, 10)
-    assert np.array_equal(ids, bi) and np.array_equal(dist, bd)
+    sc = plan == 0
+    assert np.array_equal(ids[sc], bi[sc]) and np.array_equal(dist[sc], bd[sc])
+    gsel = np.nonzero(plan > 0)[0]
+    gi, gd, gc, _ = g.graph_batch(ds.queries[gsel], ent[gsel], [preds[i] for i in gsel], 64)
+    for j, i in enumerate(gsel):
+        c = min(int(gc[j]), 10)
+        assert cnt[i] == c
+        assert np.array_equal(ids[i, :c], gi[j, :c]) and np.array_equal(dist[i, :c], gd[j, :c])
     # learned decisions equal the host rule applied to the router's logits
     rng = np.random.default_rng(2)
     p = init_params(4)
@@ -85,5 +93,5 @@ def test_mixed_plan_scans_and_router_decisions(env):
         a = r.decide(f, k, margin)
         want = np.where(a == 0, 0, np.maximum(np.array([0, 32, 64, 128, 256])[a], 10))
         assert np.array_equal(dec, want.astype(np.uint16))
-        assert ex == (1 if (want > 0).all() else 0)
+        assert ex == (1 if (want > 0).all() else 2 if (want > 0).any() else 0)
         assert (st >= 0).all()
