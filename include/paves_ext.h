@@ -253,17 +253,22 @@ int pv_router_train(PvRouter *r, int n, const float *feats, const int32_t *label
 /* Learned-routed filtered top-k batch (no reference counterpart): builds
  * the batch's predicate bitmaps, computes the router's features and MLP
  * action per query on the device, and answers each query by the route
- * chosen for it: the graph search at its beam width, or the scan of the
- * index's precision. The scan starts speculatively beside the routing (a
- * scan costs about the same for one query as for a query tile); the graph
- * search runs, on a second stream, for the graph-routed queries only, and
- * a batch whose every query went to the graph discards the scan. plan
+ * chosen for it (see split): the graph search at its beam width, or the
+ * scan of the index's precision. The scan starts speculatively beside the
+ * routing (a scan costs about the same for one query as for a query tile);
+ * the graph search runs on a second stream, and a batch whose every query
+ * went to the graph discards the scan. plan
  * (optional, replaces the router, r may then be NULL): per query 0 = scan
  * or the beam width to use. k[nq] <= topb; out has stride topb and holds
- * min(k, found) hits per query. qd[i].entry must hold the level-0 entry
+ * min(k, found) hits per query. split 0: a batch that is scanned (any
+ * query routed to the scan) answers every query from the scan, which is
+ * exact on certified data and already paid for; split 1: each query takes
+ * its own route, graph-routed ones from the graph search run beside the
+ * scan. qd[i].entry must hold the level-0 entry
  * point when the index has a graph. decided[nq] (optional) receives each
- * query's beam width (0 = scan), *executed 0 when every query was scanned,
- * 1 when every query took the graph, 2 for a mixed batch; stage_ms[3] the
+ * query's beam width (0 = scan), *executed 0 when every query was answered
+ * by the scan, 1 when every query took the graph, 2 for a split batch;
+ * stage_ms[3] the
  * device time of the bitmaps, of the routing (features, MLP, decision read
  * back; it runs beside the speculative scan) and of the search after the
  * bitmaps: the batch took stage_ms[0] + stage_ms[2]. */
@@ -271,6 +276,7 @@ int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *queries,
                     const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,
                     const uint32_t *k, uint32_t topb, const uint16_t *plan, float margin,
+                    int split,
                     FvHit *out, uint32_t *out_cnt, uint16_t *decided, int *executed,
                     float *stage_ms, char *errbuf, size_t errlen);
 

@@ -180,8 +180,8 @@ _EXT_SIGS.update({
                                   P, C.c_char_p, C.c_size_t]),
 })
 _EXT_SIGS["pv_routed_batch"] = (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int,
-                                          P, C.c_uint32, P, C.c_float, P, P, P, P, P, C.c_char_p,
-                                          C.c_size_t])
+                                          P, C.c_uint32, P, C.c_float, C.c_int, P, P, P, P, P,
+                                          C.c_char_p, C.c_size_t])
 
 PV_STREAM_MAX_K = 256
 _EXT_SIGS.update({

@@ -1,23 +1,27 @@
 // hnsw_gpu.cu — HNSW graph construction on the GPU.
 //
 // No counterpart in the reference: its builder is a CPU thread pool that
-// inserts rows one at a time (engine.cpp:698-1032). Here every level is
-// built in bulk from exact nearest neighbours instead of insertion-time
-// beam searches:
-//   1. candidates: each node's C nearest other nodes of its level, exact,
-//      from this library's own scans with the nodes themselves as queries
-//      (the BF16 tensor-core scan when its distances are certified exact,
-//      else the exact FP32 scan), batch after batch, never leaving the GPU;
-//   2. forward selection, one warp per node: candidates in ascending
+// inserts rows one at a time (engine.cpp:698-1032). Here rows are inserted
+// in batches of doubling size (2048, then as many as are already in), and
+// each batch takes exact candidates instead of insertion-time beam searches:
+//   1. candidates: each new node's C nearest nodes among all nodes inserted
+//      so far (its own batch included), exact, from this library's scans
+//      with the new nodes as queries over the prefix of the rows (the BF16
+//      tensor-core scan when its distances are certified exact, else the
+//      exact FP32 scan). Rows are in random order, so the early batches are
+//      sparse samples of the data and their lists carry the long-range
+//      links an insertion order gives a navigable graph;
+//   2. forward selection, one warp per new node: candidates in ascending
 //      distance, a candidate is kept when it is closer to the node than to
 //      every neighbour kept so far (the neighbour-selection heuristic of
 //      the HNSW paper, Malkov & Yashunin, Algorithm 4), up to R; a list
 //      left short is topped up with the closest rejected candidates;
-//   3. reverse edges: every kept edge u -> v is offered to v (in-degrees
-//      counted with atomics, a prefix sum, a scatter into per-node runs);
-//   4. final selection, one warp per node: its forward and reverse
-//      candidates are sorted together (duplicates dropped) and selected
-//      again by the same rule to R.
+//   3. reverse edges: every kept edge u -> v of a new node is offered to v
+//      (in-degrees counted with atomics, a prefix sum, a scatter into
+//      per-node runs);
+//   4. re-selection, one warp per touched node: its current list and its
+//      new reverse candidates sorted together (duplicates dropped) and
+//      selected again by the same rule to R.
 // Level 0 uses R = 2M over all rows, each level L >= 1 uses R = M over the
 // nodes whose level is >= L (a sub-index of their rows). Node levels are
 // drawn as the engine draws them (so upper levels have the usual sizes),
@@ -33,6 +37,7 @@
 #include "index.h"
 #include "paves_ext.h"
 #include "pv_internal.h"
+#include "tc_core.cuh"
 
 namespace pv {
 
@@ -77,8 +82,9 @@ __device__ __forceinline__ void hg_row(float4 (&r)[NV], const float *x, uint64_t
 }
 
 // The selection rule on n ascending candidate keys of node v (smem, warp
-// private): keeps up to R ids in kept[], topping up from rejected ones.
-// Returns the number kept. Keys equal to v's own id are skipped.
+// private): keeps up to R candidates, topping up from rejected ones; kept[]
+// receives their positions in ck. Returns the number kept. Keys of v
+// itself are skipped.
 template <int NV>
 __device__ int hg_select(const uint64_t *ck, int n, uint32_t v, int R, const float *x, int dpad,
                          uint32_t *kept, uint32_t *rej, int lane) {
@@ -91,15 +97,18 @@ __device__ int hg_select(const uint64_t *ck, int n, uint32_t v, int R, const flo
         hg_row<NV>(rc, x, c, dpad, lane);
         bool ok = true;
         for (int j = 0; j < nk && ok; j++)
-            if (hg_dist<NV>(rc, x, kept[j], dpad, lane) < dc) ok = false;
+            if (hg_dist<NV>(rc, x, key_row(ck[kept[j]]), dpad, lane) < dc) ok = false;
         if (lane == 0) {
-            if (ok) kept[nk] = c;
-            else if (nr < R) rej[nr] = c;
+            if (ok) kept[nk] = (uint32_t)i;
+            else if (nr < R) rej[nr] = (uint32_t)i;
         }
         __syncwarp();
         if (ok) nk++;
         else if (nr < R) nr++;
     }
+    // top up in ascending distance: merge of the kept and rejected positions
+    // is not needed, the rejected ones come after (keys stay sorted only
+    // within each group, and lists need no order)
     for (int i = 0; i < nr && nk < R; i++) {
         if (lane == 0) kept[nk] = rej[i];
         __syncwarp();
@@ -129,58 +138,50 @@ hg_forward_kernel(const FvHit *__restrict__ cand, const uint32_t *__restrict__ c
     __syncwarp();
     const int nk = hg_select<NV>(s_ck[warp], n, (uint32_t)v, R, x, dpad, s_kept[warp],
                                  s_rej[warp], lane);
-    // keys of the kept edges: their distances from the candidate list
-    for (int j = lane; j < nk; j += 32) {
-        const uint32_t id = s_kept[warp][j];
-        float d = 0.f;
-        for (int i = 0; i < n; i++)
-            if (key_row(s_ck[warp][i]) == id) {
-                d = key_dist(s_ck[warp][i]);
-                break;
-            }
-        fwd[v * R + j] = make_key(d, id);
-    }
+    for (int j = lane; j < nk; j += 32) fwd[v * R + j] = s_ck[warp][s_kept[warp][j]];
     if (lane == 0) fwd_cnt[v] = (uint32_t)nk;
 }
 
 // Step 3: in-degrees, then the scatter of reverse edges into per-node runs.
+// (edges of the sources [u0, u0 + nu))
 __global__ void hg_count_kernel(const uint64_t *__restrict__ fwd,
-                                const uint32_t *__restrict__ fwd_cnt, uint64_t n, int R,
-                                uint32_t *__restrict__ in_cnt) {
+                                const uint32_t *__restrict__ fwd_cnt, uint64_t u0, uint64_t nu,
+                                int R, uint32_t *__restrict__ in_cnt) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n * (uint64_t)R) return;
-    const uint64_t u = i / R;
-    if ((uint32_t)(i - u * R) >= fwd_cnt[u]) return;
-    atomicAdd(&in_cnt[key_row(fwd[i])], 1u);
+    if (i >= nu * (uint64_t)R) return;
+    const uint64_t u = u0 + i / R;
+    if ((uint32_t)(i % R) >= fwd_cnt[u]) return;
+    atomicAdd(&in_cnt[key_row(fwd[u * R + i % R])], 1u);
 }
 
 __global__ void hg_scatter_kernel(const uint64_t *__restrict__ fwd,
-                                  const uint32_t *__restrict__ fwd_cnt, uint64_t n, int R,
-                                  const uint64_t *__restrict__ in_off,
+                                  const uint32_t *__restrict__ fwd_cnt, uint64_t u0, uint64_t nu,
+                                  int R, const uint64_t *__restrict__ in_off,
                                   uint32_t *__restrict__ cursor, uint64_t *__restrict__ rev) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n * (uint64_t)R) return;
-    const uint64_t u = i / R;
-    if ((uint32_t)(i - u * R) >= fwd_cnt[u]) return;
-    const uint64_t k = fwd[i];
+    if (i >= nu * (uint64_t)R) return;
+    const uint64_t u = u0 + i / R;
+    if ((uint32_t)(i % R) >= fwd_cnt[u]) return;
+    const uint64_t k = fwd[u * R + i % R];
     const uint32_t v = key_row(k);
     const uint32_t pos = atomicAdd(&cursor[v], 1u);
     rev[in_off[v] + pos] = make_key(key_dist(k), (uint32_t)u);
 }
 
-// Step 4: final selection over forward + reverse candidates; writes the
-// list [cnt, ids...] (stride R + 1) of every node.
+// Step 4: re-selection over a node's list and its new reverse candidates,
+// for the nodes [0, n) touched by this batch (new nodes >= lo, or with
+// reverse edges); the list (keys, in place) and its count are rewritten.
 template <int NV>
 __global__ void __launch_bounds__(32 * HG_WARPS)
-hg_final_kernel(const uint64_t *__restrict__ fwd, const uint32_t *__restrict__ fwd_cnt,
+hg_final_kernel(uint64_t *__restrict__ fwd, uint32_t *__restrict__ fwd_cnt,
                 const uint64_t *__restrict__ rev, const uint64_t *__restrict__ in_off,
-                const uint32_t *__restrict__ in_cnt, uint64_t n, int R,
-                const float *__restrict__ x, int dpad, uint32_t *__restrict__ lists) {
+                const uint32_t *__restrict__ in_cnt, uint64_t n, uint64_t lo, int R,
+                const float *__restrict__ x, int dpad) {
     __shared__ uint64_t s_ck[HG_WARPS][HG_CAP];
     __shared__ uint32_t s_kept[HG_WARPS][HG_RMAX], s_rej[HG_WARPS][HG_RMAX];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t v = (uint64_t)blockIdx.x * HG_WARPS + warp;
-    if (v >= n) return;
+    if (v >= n || (v < lo && in_cnt[v] == 0)) return;
     uint64_t *ck = s_ck[warp];
     const int nf = (int)fwd_cnt[v];
     // reverse runs longer than the buffer keep their first entries (rare:
@@ -224,9 +225,20 @@ hg_final_kernel(const uint64_t *__restrict__ fwd, const uint32_t *__restrict__ f
         __syncwarp();
     }
     const int nk = hg_select<NV>(ck, m, (uint32_t)v, R, x, dpad, s_kept[warp], s_rej[warp], lane);
-    uint32_t *dst = lists + v * (uint64_t)(R + 1);
-    for (int j = lane; j < R; j += 32) dst[1 + j] = j < nk ? s_kept[warp][j] : 0u;
-    if (lane == 0) dst[0] = (uint32_t)nk;
+    for (int j = lane; j < nk; j += 32) fwd[v * R + j] = ck[s_kept[warp][j]];
+    if (lane == 0) fwd_cnt[v] = (uint32_t)nk;
+}
+
+// The lists in the file layout: [cnt, ids...] of stride R + 1.
+__global__ void hg_export_kernel(const uint64_t *__restrict__ lst,
+                                 const uint32_t *__restrict__ cnt, uint64_t n, int R,
+                                 uint32_t *__restrict__ lists) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * (uint64_t)(R + 1)) return;
+    const uint64_t v = i / (R + 1);
+    const int j = (int)(i % (R + 1));
+    const uint32_t c = cnt[v];
+    lists[i] = j == 0 ? c : (uint32_t)(j - 1) < c ? key_row(lst[v * R + j - 1]) : 0u;
 }
 
 namespace {
@@ -261,11 +273,11 @@ void launch_forward(const FvHit *cand, const uint32_t *ccnt, int topb, uint64_t 
         cand, ccnt, topb, n0, nq, R, x, dpad, fwd, fwd_cnt);
 }
 template <int NV>
-void launch_final(const uint64_t *fwd, const uint32_t *fwd_cnt, const uint64_t *rev,
-                  const uint64_t *in_off, const uint32_t *in_cnt, uint64_t n, int R,
-                  const float *x, int dpad, uint32_t *lists, cudaStream_t st) {
+void launch_final(uint64_t *fwd, uint32_t *fwd_cnt, const uint64_t *rev, const uint64_t *in_off,
+                  const uint32_t *in_cnt, uint64_t n, uint64_t lo, int R, const float *x,
+                  int dpad, cudaStream_t st) {
     hg_final_kernel<NV><<<(unsigned)((n + HG_WARPS - 1) / HG_WARPS), 32 * HG_WARPS, 0, st>>>(
-        fwd, fwd_cnt, rev, in_off, in_cnt, n, R, x, dpad, lists);
+        fwd, fwd_cnt, rev, in_off, in_cnt, n, lo, R, x, dpad);
 }
 
 // Exact nearest neighbours of rows [r0, r0 + nq) of g among all rows of g:
@@ -320,81 +332,124 @@ int knn_batch(FvGpuIndex *g, uint64_t r0, int nq, uint32_t topb, const int32_t *
     return 0;
 }
 
-// One level over the rows of g: lists [count][R + 1] (device) of local ids.
+// One level over the rows of g by batched insertion: lists [count][R + 1]
+// (device) of local ids.
 int build_level(FvGpuIndex *g, int R, int C, uint32_t *d_lists, char *errbuf, size_t errlen) {
     const uint64_t n = g->count;
     const int dpad = g->dpad;
     const int NVn = (dpad + 127) / 128;
-    const int topb = (int)std::min<uint64_t>((uint64_t)C + 1, n);  // self included
-    const int B = 2048;
+    const int B = 2048;          // scan batch (queries per call)
+    const uint64_t first = 2048;  // first insertion batch
     cudaStream_t st = g->stream;
-    DevArr qprog, popcnt, out, cnt, tr, fwd, fwd_cnt, in_cnt, in_off, cursor, rev;
+    // the rows' tensor map covers all rows, whatever prefix is scanned
+    if (g->precision != FV_GPU_PREC_FP32 && !g->tmap_x_ok) {
+        CUtensorMap m;
+        if (!tc_make_tmap(&m, g->d_vlow, g->precision == FV_GPU_PREC_FP8, (uint64_t)g->kpad,
+                          g->count)) {
+            snprintf(errbuf, errlen, "hnsw gpu: tensor map encoding failed");
+            return -1;
+        }
+        memcpy(g->tmap_x, &m, sizeof(m));
+        g->tmap_x_ok = true;
+    }
+    DevArr qprog, popcnt, out, cnt, tr, lst, lcnt, in_cnt, in_off, cursor, rev;
+    const int topb_max = (int)std::min<uint64_t>((uint64_t)C + 1, n);  // self included
     HG_OK(qprog.alloc((size_t)B * 4));
     HG_OK(cudaMemsetAsync(qprog.p, 0xFF, (size_t)B * 4, st));  // no filter
     HG_OK(popcnt.alloc(8));
-    HG_OK(out.alloc((size_t)B * topb * sizeof(FvHit)));
+    HG_OK(out.alloc((size_t)B * topb_max * sizeof(FvHit)));
     HG_OK(cnt.alloc((size_t)B * 4));
     HG_OK(tr.alloc((size_t)B));
-    HG_OK(fwd.alloc((size_t)n * R * 8));
-    HG_OK(fwd_cnt.alloc((size_t)n * 4));
-    for (uint64_t r0 = 0; r0 < n; r0 += B) {
-        const int nq = (int)std::min<uint64_t>(B, n - r0);
-        if (knn_batch(g, r0, nq, (uint32_t)topb, qprog.as<int32_t>(),
-                      popcnt.as<unsigned long long>(), out.as<FvHit>(), cnt.as<uint32_t>(),
-                      tr.as<uint8_t>(), errbuf, errlen))
-            return -1;
-        if (NVn <= 1)
-            launch_forward<1>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
-                              dpad, fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), st);
-        else if (NVn <= 2)
-            launch_forward<2>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
-                              dpad, fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), st);
-        else
-            launch_forward<4>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
-                              dpad, fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), st);
-        HG_OK(cudaGetLastError());
-    }
-    if (int rc = check_tc_watchdog(g, errbuf, errlen)) return rc;
-    // reverse edges
+    HG_OK(lst.alloc((size_t)n * R * 8));
+    HG_OK(lcnt.alloc((size_t)n * 4));
     HG_OK(in_cnt.alloc((size_t)n * 4));
     HG_OK(cursor.alloc((size_t)n * 4));
     HG_OK(in_off.alloc((size_t)(n + 1) * 8));
-    HG_OK(cudaMemsetAsync(in_cnt.p, 0, (size_t)n * 4, st));
-    HG_OK(cudaMemsetAsync(cursor.p, 0, (size_t)n * 4, st));
-    const uint64_t edges = n * (uint64_t)R;
-    const unsigned eb = (unsigned)((edges + 255) / 256);
-    hg_count_kernel<<<eb, 256, 0, st>>>(fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), n, R,
-                                        in_cnt.as<uint32_t>());
-    HG_OK(cudaGetLastError());
-    std::vector<uint32_t> h_in(n);
-    std::vector<uint64_t> h_off(n + 1);
-    HG_OK(cudaMemcpyAsync(h_in.data(), in_cnt.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
-    HG_OK(cudaStreamSynchronize(st));
-    uint64_t tot = 0;
-    for (uint64_t i = 0; i < n; i++) {
-        h_off[i] = tot;
-        tot += h_in[i];
+    HG_OK(cudaMemsetAsync(lcnt.p, 0, (size_t)n * 4, st));
+    std::vector<uint32_t> h_in;
+    std::vector<uint64_t> h_off;
+    size_t rev_cap = 0;
+    int rc = 0;
+    for (uint64_t lo = 0; lo < n && rc == 0;) {
+        const uint64_t hi = lo == 0 ? std::min(n, first) : std::min(n, 2 * lo);
+        // 1-2: candidates among the inserted prefix [0, hi), forward selection
+        g->count = hi;
+        const int topb = (int)std::min<uint64_t>((uint64_t)C + 1, hi);
+        for (uint64_t r0 = lo; r0 < hi && rc == 0; r0 += B) {
+            const int nq = (int)std::min<uint64_t>(B, hi - r0);
+            rc = knn_batch(g, r0, nq, (uint32_t)topb, qprog.as<int32_t>(),
+                           popcnt.as<unsigned long long>(), out.as<FvHit>(), cnt.as<uint32_t>(),
+                           tr.as<uint8_t>(), errbuf, errlen);
+            if (rc) break;
+            if (NVn <= 1)
+                launch_forward<1>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
+                                  dpad, lst.as<uint64_t>(), lcnt.as<uint32_t>(), st);
+            else if (NVn <= 2)
+                launch_forward<2>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
+                                  dpad, lst.as<uint64_t>(), lcnt.as<uint32_t>(), st);
+            else
+                launch_forward<4>(out.as<FvHit>(), cnt.as<uint32_t>(), topb, r0, nq, R, g->d_vecs,
+                                  dpad, lst.as<uint64_t>(), lcnt.as<uint32_t>(), st);
+            if (cudaGetLastError() != cudaSuccess) rc = -1;
+        }
+        g->count = n;
+        if (rc) break;
+        if ((rc = check_tc_watchdog(g, errbuf, errlen))) break;
+        // 3: reverse edges of the new nodes' lists
+        const uint64_t nu = hi - lo;
+        HG_OK(cudaMemsetAsync(in_cnt.p, 0, (size_t)hi * 4, st));
+        HG_OK(cudaMemsetAsync(cursor.p, 0, (size_t)hi * 4, st));
+        const unsigned eb = (unsigned)((nu * R + 255) / 256);
+        hg_count_kernel<<<eb, 256, 0, st>>>(lst.as<uint64_t>(), lcnt.as<uint32_t>(), lo, nu, R,
+                                            in_cnt.as<uint32_t>());
+        HG_OK(cudaGetLastError());
+        h_in.resize(hi);
+        h_off.resize(hi + 1);
+        HG_OK(cudaMemcpyAsync(h_in.data(), in_cnt.p, (size_t)hi * 4, cudaMemcpyDeviceToHost, st));
+        HG_OK(cudaStreamSynchronize(st));
+        uint64_t tot = 0;
+        for (uint64_t i = 0; i < hi; i++) {
+            h_off[i] = tot;
+            tot += h_in[i];
+        }
+        h_off[hi] = tot;
+        HG_OK(cudaMemcpyAsync(in_off.p, h_off.data(), (size_t)(hi + 1) * 8,
+                              cudaMemcpyHostToDevice, st));
+        if (tot > rev_cap) {
+            if (rev.p) {
+                HG_OK(cudaStreamSynchronize(st));
+                cudaFree(rev.p);
+                rev.p = nullptr;
+            }
+            HG_OK(rev.alloc((size_t)tot * 8));
+            rev_cap = tot;
+        }
+        hg_scatter_kernel<<<eb, 256, 0, st>>>(lst.as<uint64_t>(), lcnt.as<uint32_t>(), lo, nu, R,
+                                              in_off.as<uint64_t>(), cursor.as<uint32_t>(),
+                                              rev.as<uint64_t>());
+        HG_OK(cudaGetLastError());
+        // 4: re-selection of every touched list
+        if (NVn <= 1)
+            launch_final<1>(lst.as<uint64_t>(), lcnt.as<uint32_t>(), rev.as<uint64_t>(),
+                            in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), hi, lo, R, g->d_vecs,
+                            dpad, st);
+        else if (NVn <= 2)
+            launch_final<2>(lst.as<uint64_t>(), lcnt.as<uint32_t>(), rev.as<uint64_t>(),
+                            in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), hi, lo, R, g->d_vecs,
+                            dpad, st);
+        else
+            launch_final<4>(lst.as<uint64_t>(), lcnt.as<uint32_t>(), rev.as<uint64_t>(),
+                            in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), hi, lo, R, g->d_vecs,
+                            dpad, st);
+        HG_OK(cudaGetLastError());
+        HG_OK(cudaStreamSynchronize(st));  // rev and the host offsets are reused next batch
+        lo = hi;
     }
-    h_off[n] = tot;
-    HG_OK(cudaMemcpyAsync(in_off.p, h_off.data(), (size_t)(n + 1) * 8, cudaMemcpyHostToDevice,
-                          st));
-    HG_OK(rev.alloc((size_t)tot * 8));
-    hg_scatter_kernel<<<eb, 256, 0, st>>>(fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), n, R,
-                                          in_off.as<uint64_t>(), cursor.as<uint32_t>(),
-                                          rev.as<uint64_t>());
-    HG_OK(cudaGetLastError());
-    if (NVn <= 1)
-        launch_final<1>(fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), rev.as<uint64_t>(),
-                        in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), n, R, g->d_vecs, dpad,
-                        d_lists, st);
-    else if (NVn <= 2)
-        launch_final<2>(fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), rev.as<uint64_t>(),
-                        in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), n, R, g->d_vecs, dpad,
-                        d_lists, st);
-    else
-        launch_final<4>(fwd.as<uint64_t>(), fwd_cnt.as<uint32_t>(), rev.as<uint64_t>(),
-                        in_off.as<uint64_t>(), in_cnt.as<uint32_t>(), n, R, g->d_vecs, dpad,
-                        d_lists, st);
+    g->count = n;
+    if (rc) return -1;
+    const uint64_t total = n * (uint64_t)(R + 1);
+    hg_export_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        lst.as<uint64_t>(), lcnt.as<uint32_t>(), n, R, d_lists);
     HG_OK(cudaGetLastError());
     HG_OK(cudaStreamSynchronize(st));
     return 0;

@@ -125,6 +125,11 @@ int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &p
 inline uint64_t sparse_limit(uint64_t nrows) { return nrows / 16 > 4096 ? nrows / 16 : 4096; }
 void build_sorted_cols(FvGpuIndex *g, const double *cols, const uint32_t *post_rows);
 uint64_t prog_upper_bound(const FvGpuIndex *g, const PredInsn *ins, int n, const double *consts);
+double prog_pass_estimate(const FvGpuIndex *g, const PredInsn *ins, int n, const double *consts);
+// lazy filters pay one filter test per row that beats the threshold; a
+// selective filter leaves a loose threshold (few passing rows), so only
+// programs estimated to pass at least this fraction are tested lazily
+constexpr double PV_LAZY_MIN_PASS = 0.125;
 int sparse_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, FvHit *d_out,
                   uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen);
 int tc_redo_uncertain(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,

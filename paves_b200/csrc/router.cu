@@ -849,7 +849,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                                const FvGpuQueryDesc *qd, const FvGpuPredNode *nodes, int nnodes,
                                const int32_t *children, int nchildren, const double *invals,
                                int ninvals, const uint32_t *k, uint32_t topb,
-                               const uint16_t *plan, float margin, FvHit *out,
+                               const uint16_t *plan, float margin, int split, FvHit *out,
                                uint32_t *out_cnt, uint16_t *decided, int *executed,
                                float *stage_ms, char *errbuf, size_t errlen) {
     if (!g || nq < 1 || nq > FV_GPU_MAX_BATCH || !queries || !qd || !k || !out || !out_cnt ||
@@ -989,6 +989,13 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     }
     const bool all_graph = have_graph && ngraph == nq;
     if (decided) memcpy(decided, hefq, (size_t)nq * 2);
+    if (!split && !all_graph && spec) {
+        // a batch that is scanned anyway answers every query from the scan
+        // (exact, and already paid for); graph-routed queries in it would
+        // only add the graph's time
+        for (int i = 0; i < nq; i++) hefq[i] = 0;
+        ngraph = 0;
+    }
     if (executed) *executed = ngraph == 0 ? 0 : all_graph ? 1 : 2;
     if (!spec && !all_graph) {  // a plan sent every query to a graph the index lacks
         if (errbuf && errlen) snprintf(errbuf, errlen, "routed: no graph for the plan");

@@ -85,51 +85,6 @@ namespace pv {
 // Row qi holds query qi % bq (bq = nqpad without replication). Also resets
 // the scan's per-query state for query qi < nq: bound tau (none), dense run
 // count, full-list minimum (if tracked), and the watchdog word.
-// one warp: query row qi of the tile (qi < nqpad)
-__device__ __forceinline__ void query_prep_row(int qi, int lane, const float *__restrict__ q,
-                                               int nq, int dpad, int dim, int bq, int kelems,
-                                               bool fp8, unsigned char *__restrict__ out,
-                                               float *__restrict__ qnorm,
-                                               float *__restrict__ qscale,
-                                               unsigned long long *__restrict__ tau,
-                                               uint32_t *__restrict__ dcnt,
-                                               unsigned long long *__restrict__ fullmin,
-                                               int *__restrict__ err) {
-    if (lane == 0 && qi < nq) {
-        tau[qi] = KEY_MAX;
-        dcnt[qi] = 0;
-        if (fullmin) fullmin[qi] = KEY_MAX;
-        if (qi == 0) *err = 0;
-    }
-    const int src = qi % bq;
-    const bool ok = src < nq;
-    float amax = 0.f;
-    if (fp8 && ok)
-        for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(q[(size_t)src * dpad + j]));
-    for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    const float s = amax > 0.f ? amax / 448.f : 1.f;
-    float acc = 0.f;
-    for (int j = lane; j < kelems; j += 32) {
-        const float v = (ok && j < dim) ? q[(size_t)src * dpad + j] : 0.f;
-        float r;
-        if (fp8) {
-            __nv_fp8_e4m3 b(v / s);
-            out[(size_t)qi * kelems + j] = *(unsigned char *)&b;
-            r = float(b) * s;
-        } else {
-            __nv_bfloat16 b = __float2bfloat16_rn(v);
-            ((__nv_bfloat16 *)out)[(size_t)qi * kelems + j] = b;
-            r = __bfloat162float(b);
-        }
-        acc = fmaf(r, r, acc);
-    }
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
-        qnorm[qi] = acc;
-        if (qscale) qscale[qi] = s;
-    }
-}
-
 __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad, int dim,
                                   int nqpad, int bq, int kelems, bool fp8,
                                   unsigned char *__restrict__ out, float *__restrict__ qnorm,
@@ -147,78 +102,6 @@ __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad,
 // (up to TC_MAX_SUPERSET, row stride S); keeps the best topb by (dist, id).
 // One CTA (8 warps) per query: 8 lanes per candidate, 32 candidates in
 // flight, then a bitonic sort of the keys in shared memory.
-// One query's re-rank by the block's NT threads (8 lanes per candidate,
-// NT / 8 in flight); keys: TC_MAX_SUPERSET slots of shared memory. Ends
-// with the block synchronized.
-template <int NT>
-__device__ __forceinline__ void rerank_query(int q, uint64_t *keys, const float *__restrict__ vecs,
-                                             int dpad, const float *__restrict__ queries,
-                                             const FvHit *__restrict__ cand,
-                                             const uint32_t *__restrict__ cand_cnt, int S,
-                                             uint32_t topb, const int32_t *__restrict__ qprog,
-                                             const unsigned long long *__restrict__ popcnt,
-                                             uint64_t nrows, FvHit *__restrict__ out,
-                                             uint32_t *__restrict__ out_cnt,
-                                             uint8_t *__restrict__ trunc) {
-    const int tid = threadIdx.x;
-    const int grp = tid >> 3, sub = tid & 7;
-    int n = (int)cand_cnt[q];
-    if (n > S) n = S;
-    const float *qv = queries + (size_t)q * dpad;
-    for (int base = 0; base < n; base += NT / 8) {
-        const int j = base + grp;
-        const bool ok = j < n;
-        const uint32_t row = (uint32_t)cand[(size_t)q * S + (ok ? j : 0)].node;
-        const float *x = vecs + (size_t)row * dpad;
-        float acc = 0.f;
-        for (int k = sub * 4; k < dpad; k += 32) {
-            const float4 v = __ldg((const float4 *)(x + k));
-            const float4 w = __ldg((const float4 *)(qv + k));
-            const float d0 = v.x - w.x, d1 = v.y - w.y, d2 = v.z - w.z, d3 = v.w - w.w;
-            acc = fmaf(d0, d0, acc);
-            acc = fmaf(d1, d1, acc);
-            acc = fmaf(d2, d2, acc);
-            acc = fmaf(d3, d3, acc);
-        }
-        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        if (ok && sub == 0) keys[j] = make_key(acc, row);
-    }
-    int n2 = 1;
-    while (n2 < n) n2 <<= 1;
-    for (int i = n + tid; i < n2; i += blockDim.x) keys[i] = KEY_MAX;
-    __syncthreads();
-    for (int k = 2; k <= n2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = tid; i < (n2 >> 1); i += blockDim.x) {
-                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-                const int hi = lo | j;
-                const uint64_t x = keys[lo], y = keys[hi];
-                if ((x > y) == ((lo & k) == 0)) {
-                    keys[lo] = y;
-                    keys[hi] = x;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    const int nout = n < (int)topb ? n : (int)topb;
-    for (int i = tid; i < nout; i += blockDim.x) {
-        FvHit h;
-        h.node = key_row(keys[i]);
-        h.dist = key_dist(keys[i]);
-        out[(size_t)q * topb + i] = h;
-    }
-    if (tid == 0) {
-        out_cnt[q] = (uint32_t)nout;
-        const int pg = qprog[q];
-        const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
-        trunc[q] = passing > (unsigned long long)topb ? 1 : 0;
-    }
-    __syncthreads();
-}
-
 __global__ void __launch_bounds__(256)
 rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict__ queries,
               const FvHit *__restrict__ cand, const uint32_t *__restrict__ cand_cnt, int S,
@@ -241,181 +124,6 @@ rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict_
 // below it are sorted. Runs up to stage_cap keys are staged in shared
 // memory; longer ones are read from global memory on every pass (4 loads
 // in flight per lane).
-constexpr int DM_THREADS = 512;
-constexpr int DM_CAP_MAX = 24576;   // largest shared-memory stage
-constexpr int DM_OUT = TC_MAX_SUPERSET;
-
-__device__ __forceinline__ void dm_hist_add(unsigned *hist, bool act, unsigned d, int lane) {
-    const int tag = act ? (int)d : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, tag);
-    if (act && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (unsigned)__popc(peers));
-}
-
-// One query's merge (radix select, any KO <= DM_OUT) by all threads of the
-// block; smem_keys: stage_cap + DM_OUT keys of shared memory. Ends with the
-// block synchronized.
-__device__ __noinline__ void dense_merge_query(
-    int q, uint64_t *smem_keys, const uint64_t *__restrict__ dense, uint64_t dcap, int stage_cap,
-    uint32_t *__restrict__ dcnt, int reset_cnt, const unsigned long long *__restrict__ fullmin,
-    const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
-    const unsigned long long *__restrict__ popcnt, uint64_t nrows, FvHit *__restrict__ out,
-    uint32_t *__restrict__ out_cnt, uint8_t *__restrict__ trunc, unsigned long long *tau_out,
-    uint8_t *__restrict__ unc) {
-    uint64_t *buf = smem_keys;        // [stage_cap] staged keys
-    uint64_t *res = buf + stage_cap;  // [DM_OUT] the answer, sorted
-    __shared__ unsigned hist[256];
-    __shared__ int s_m, s_c, s_digit, s_rank, s_tot;
-    const int NW = blockDim.x >> 5;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const unsigned long long bound = tau ? tau[q] : KEY_MAX;
-    uint64_t n = dcnt[q];
-    if (n > dcap) n = dcap;
-    const uint64_t *src = dense + (uint64_t)q * dcap;
-    if (tid == 0) {
-        s_m = 0;
-        s_c = 0;
-    }
-    __syncthreads();
-    if (reset_cnt && tid == 0) dcnt[q] = 0;  // every thread has read it
-    const bool staged = n <= (uint64_t)stage_cap;
-    if (staged) {
-        for (uint64_t b = (uint64_t)warp * 32; b < n; b += NW * 32) {
-            const uint64_t i = b + lane;
-            const uint64_t key = i < n ? src[i] : KEY_MAX;
-            const bool keep = i < n && key <= bound;
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            int base = 0;
-            if (lane == 0 && bal) base = atomicAdd(&s_m, __popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) buf[base + __popc(bal & ((1u << lane) - 1u))] = key;
-        }
-    }
-    __syncthreads();
-    // candidates: buf[0, s_m) if staged, else the keys <= bound of src[0, n)
-    const uint64_t N = staged ? (uint64_t)s_m : n;
-    uint64_t kth = KEY_MAX;  // keep every candidate unless there are more than KO
-    if (!staged || s_m > KO) {
-        uint64_t prefix = 0;
-        int rank = KO;
-        bool selected = true;
-        for (int pass = 0; pass < 8; pass++) {
-            const int shift = 56 - 8 * pass;
-            for (int i = tid; i < 256; i += (int)blockDim.x) hist[i] = 0;
-            __syncthreads();
-            for (uint64_t b = (uint64_t)warp * 128; b < N; b += NW * 128) {
-                uint64_t key[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const uint64_t i = b + u * 32 + lane;
-                    key[u] = i < N ? (staged ? buf[i] : src[i]) : KEY_MAX;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    bool act = b + u * 32 + lane < N && (staged || key[u] <= bound);
-                    if (pass > 0) act = act && (key[u] >> (shift + 8)) == (prefix >> (shift + 8));
-                    dm_hist_add(hist, act, (unsigned)(key[u] >> shift) & 255u, lane);
-                }
-            }
-            __syncthreads();
-            if (warp == 0) {
-                unsigned c[8], sum = 0;
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    c[j] = hist[lane * 8 + j];
-                    sum += c[j];
-                }
-                unsigned incl = sum;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += v;
-                }
-                const unsigned excl = incl - sum;
-                if (pass == 0 && lane == 31) s_tot = (int)incl;
-                if (excl < (unsigned)rank && (unsigned)rank <= incl) {
-                    unsigned cum = excl;
-                    int j = 0;
-                    for (; j < 7; j++) {
-                        if (cum + c[j] >= (unsigned)rank) break;
-                        cum += c[j];
-                    }
-                    s_digit = lane * 8 + j;
-                    s_rank = rank - (int)cum;
-                }
-            }
-            __syncthreads();
-            if (pass == 0 && s_tot <= KO) {  // no more than KO candidates
-                selected = false;
-                break;
-            }
-            prefix |= (uint64_t)s_digit << shift;
-            rank = s_rank;
-        }
-        if (selected) kth = prefix;
-    }
-    // the answer: candidates <= kth (exactly min(count, KO) keys)
-    for (uint64_t b = (uint64_t)warp * 128; b < N; b += NW * 128) {
-        uint64_t key[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const uint64_t i = b + u * 32 + lane;
-            key[u] = i < N ? (staged ? buf[i] : src[i]) : KEY_MAX;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const bool keep = b + u * 32 + lane < N && key[u] <= bound && key[u] <= kth;
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            int base = 0;
-            if (lane == 0 && bal) base = atomicAdd(&s_c, __popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            const int pos = base + __popc(bal & ((1u << lane) - 1u));
-            if (keep && pos < DM_OUT) res[pos] = key[u];
-        }
-    }
-    __syncthreads();
-    const int c = min(min(s_c, KO), DM_OUT);
-    int n2 = 1;
-    while (n2 < c) n2 <<= 1;
-    for (int i = c + tid; i < n2; i += (int)blockDim.x) res[i] = KEY_MAX;
-    __syncthreads();
-    for (int k = 2; k <= n2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = tid; i < (n2 >> 1); i += (int)blockDim.x) {
-                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-                const int hi = lo | j;
-                const uint64_t x = res[lo], y = res[hi];
-                if ((x > y) == ((lo & k) == 0)) {
-                    res[lo] = y;
-                    res[hi] = x;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    for (int i = tid; i < c; i += (int)blockDim.x) {
-        FvHit h;
-        h.node = (uint64_t)key_row(res[i]);
-        h.dist = key_dist(res[i]);
-        out[(uint64_t)q * KO + i] = h;
-    }
-    if (tid == 0) {
-        out_cnt[q] = (uint32_t)c;
-        const int pg = qprog[q];
-        const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
-        trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
-        // the KO-th merged key bounds the KO-th key of any superset of rows
-        if (tau_out && c == KO && res[KO - 1] < tau_out[q]) tau_out[q] = res[KO - 1];
-        if (unc) {
-            // a full list whose last key is at or below the answer's last key
-            // (or the bound while the answer is short) may have dropped a
-            // member of it
-            const unsigned long long lim = c == KO ? res[KO - 1] : bound;
-            const unsigned long long fm = fullmin ? fullmin[q] : KEY_MAX;
-            unc[q] = (fm != KEY_MAX && fm <= lim) ? 1 : 0;
-        }
-    }
-    __syncthreads();
-}
-
 __global__ void __launch_bounds__(DM_THREADS)
 dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, int stage_cap,
                    uint32_t *__restrict__ dcnt, int reset_cnt,
@@ -428,104 +136,6 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, int stage_
     extern __shared__ __align__(16) unsigned char dm_smem[];
     dense_merge_query(blockIdx.x, (uint64_t *)dm_smem, dense, dcap, stage_cap, dcnt, reset_cnt,
                       fullmin, tau, KO, qprog, popcnt, nrows, out, out_cnt, trunc, tau_out, unc);
-}
-
-// The same for KO <= 32, without block barriers in the hot loop: each warp
-// keeps its 32 best keys sorted across its lanes (one key per lane) and
-// folds in 32 new keys at a time (a shuffle bitonic sort of the new keys in
-// descending order, an elementwise min with the list, which leaves the 32
-// smallest as a bitonic sequence, and a bitonic clean back to ascending);
-// a batch none of whose keys beats the list's last key is skipped. Warp 0
-// then folds the other warps' lists into its own.
-__device__ __forceinline__ uint64_t warp_sort32(uint64_t x, int lane, bool descending) {
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const uint64_t o = __shfl_xor_sync(0xffffffffu, x, j);
-            const bool up = ((lane & k) == 0) != descending;
-            const bool lower = (lane & j) == 0;
-            x = (lower == up) ? (x < o ? x : o) : (x > o ? x : o);
-        }
-    return x;
-}
-
-__device__ __forceinline__ uint64_t warp_clean32(uint64_t x, int lane) {
-#pragma unroll
-    for (int j = 16; j > 0; j >>= 1) {
-        const uint64_t o = __shfl_xor_sync(0xffffffffu, x, j);
-        x = (lane & j) == 0 ? (x < o ? x : o) : (x > o ? x : o);
-    }
-    return x;
-}
-
-// One query's merge for KO <= 32 by all threads of the block (any whole
-// number of warps); lists: one 32-key slot per warp in shared memory.
-// Ends with the block synchronized.
-__device__ __forceinline__ void dense_top32_query(
-    int q, uint64_t (*lists)[32], const uint64_t *__restrict__ dense, uint64_t dcap,
-    uint32_t *__restrict__ dcnt, int reset_cnt, const unsigned long long *__restrict__ fullmin,
-    const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
-    const unsigned long long *__restrict__ popcnt, uint64_t nrows, FvHit *__restrict__ out,
-    uint32_t *__restrict__ out_cnt, uint8_t *__restrict__ trunc, unsigned long long *tau_out,
-    uint8_t *__restrict__ unc) {
-    const int NW = blockDim.x >> 5;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const unsigned long long bound = tau ? tau[q] : KEY_MAX;
-    uint64_t n = dcnt[q];
-    if (n > dcap) n = dcap;
-    const uint64_t *src = dense + (uint64_t)q * dcap;
-    __syncthreads();
-    if (reset_cnt && tid == 0) dcnt[q] = 0;  // every thread has read it
-    uint64_t best = KEY_MAX;  // ascending across the lanes
-    for (uint64_t b = (uint64_t)warp * 64; b < n; b += NW * 64) {
-        uint64_t k2[2];
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const uint64_t i = b + u * 32 + lane;
-            k2[u] = i < n ? src[i] : KEY_MAX;
-            if (k2[u] > bound) k2[u] = KEY_MAX;
-        }
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const uint64_t worst = __shfl_sync(0xffffffffu, best, 31);
-            if (!__any_sync(0xffffffffu, k2[u] < worst)) continue;
-            const uint64_t d = warp_sort32(k2[u], lane, true);
-            best = warp_clean32(best < d ? best : d, lane);
-        }
-    }
-    lists[warp][lane] = best;
-    __syncthreads();
-    if (warp == 0) {
-        for (int w = 1; w < NW; w++) {
-            const uint64_t d = lists[w][31 - lane];  // descending
-            const uint64_t m = best < d ? best : d;
-            if (!__any_sync(0xffffffffu, m != best)) continue;
-            best = warp_clean32(m, lane);
-        }
-        const bool have = lane < KO && best != KEY_MAX;
-        const int c = __popc(__ballot_sync(0xffffffffu, have));
-        if (have) {
-            FvHit h;
-            h.node = (uint64_t)key_row(best);
-            h.dist = key_dist(best);
-            out[(uint64_t)q * KO + lane] = h;
-        }
-        const uint64_t last = __shfl_sync(0xffffffffu, best, KO - 1);
-        if (lane == 0) {
-            out_cnt[q] = (uint32_t)c;
-            const int pg = qprog[q];
-            const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
-            trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
-            if (tau_out && c == KO && last < tau_out[q]) tau_out[q] = last;
-            if (unc) {
-                const unsigned long long lim = c == KO ? last : bound;
-                const unsigned long long fm = fullmin ? fullmin[q] : KEY_MAX;
-                unc[q] = (fm != KEY_MAX && fm <= lim) ? 1 : 0;
-            }
-        }
-    }
-    __syncthreads();
 }
 
 __global__ void __launch_bounds__(DM_THREADS)
@@ -582,7 +192,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 
 // 2-D row-major [rows][inner] tensor map with 128-byte swizzled boxes of
 // [128 rows][128 bytes].
-static bool make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner, uint64_t rows) {
+bool tc_make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner, uint64_t rows) {
     auto enc = get_encode();
     if (!enc) return false;
     const uint32_t esz = fp8 ? 1 : 2;
@@ -735,7 +345,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
     if (!g->tmap_x_ok) {
-        if (!make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count)) {
+        if (!tc_make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count)) {
             snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
             return -1;
         }
@@ -744,7 +354,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     }
     memcpy(&tmX, g->tmap_x, sizeof(tmX));
     if (g->tmap_q_ptr != c || g->tmap_q_rows != (uint64_t)nqpad) {
-        if (!make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
+        if (!tc_make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
             g->tmap_q_ptr = nullptr;
             snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
             return -1;
@@ -827,8 +437,9 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         // keeps the merge cheap (the radix select of S > 32 reads its run
         // 8 times). The sample's S best keys are spread over many lists
         // (S / nlists per list on average), so a list rarely holds more
-        // than two of them: 4S keys in all, at least two per list.
-        sa.kwrite = std::max(2, std::min(KP, (4 * S + nlists - 1) / std::max(1, nlists)));
+        // than two of them: 4S keys in all, at least two per list, never
+        // more than the main pass's list length (its shared memory).
+        sa.kwrite = std::min(KP, std::max(2, (4 * S + nlists - 1) / std::max(1, nlists)));
         // lists need hold no more than that (short heaps admit fewer rows);
         // a full list's last key bounds the S-th key only if it holds S
         sa.KP = sa.kwrite;

@@ -59,6 +59,42 @@ uint64_t count_cmp(const std::vector<double> &v, int op, double c) {
 
 }  // namespace
 
+// Estimated fraction of rows a range-form program passes: the product of
+// its terms' exact fractions (independent columns); 0 for other programs or
+// without sorted columns.
+double prog_pass_estimate(const FvGpuIndex *g, const PredInsn *ins, int n, const double *consts) {
+    if (n != 1 || ins[0].kind != PV_NODE_RANGE || g->count == 0 ||
+        (int)g->sorted_cols.size() != g->ncols)
+        return 0.0;
+    const double N = (double)g->count;
+    double f = 1.0;
+    int ci = ins[0].val0;
+    for (int k = 0; k < ins[0].n; k++) {
+        const int meta = (int)consts[ci];
+        const int col = meta & 0xFFFF;
+        if (col >= g->ncols) return 0.0;
+        const std::vector<double> &v = g->sorted_cols[col];
+        uint64_t c = 0;
+        if (meta & PV_TERM_MASK) {
+            uint64_t bits;
+            memcpy(&bits, &consts[ci + 1], 8);
+            for (int b = 0; b < 64; b++)
+                if ((bits >> b) & 1ull) c += count_cmp(v, FV_CMP_EQ, (double)b);
+            ci += 2;
+        } else {
+            const double lo = consts[ci + 1], hi = consts[ci + 2];
+            if (lo == lo && hi == hi) {
+                const uint64_t a = std::lower_bound(v.begin(), v.end(), lo) - v.begin();
+                const uint64_t b = std::upper_bound(v.begin(), v.end(), hi) - v.begin();
+                c = b > a ? b - a : 0;
+            }
+            ci += 3;
+        }
+        f *= (double)c / N;
+    }
+    return f;
+}
+
 uint64_t prog_upper_bound(const FvGpuIndex *g, const PredInsn *ins, int n, const double *consts) {
     const uint64_t N = g->count;
     if ((int)g->sorted_cols.size() != g->ncols || g->ncols == 0) return N;

@@ -112,7 +112,8 @@ int alloc(Bucket &b, char *errbuf, size_t errlen) {
 // Writes nq queries (padded to B by repeating the last) and the compiled
 // predicates into the bucket's staging buffer. Returns 1 if the predicates
 // exceed the bucket's capacities.
-int stage(Bucket &b, const FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb) {
+int stage(Bucket &b, const FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
+          const FvGpuIndex *owner = nullptr) {
     const int P = (int)pb.progs.size();
     if (P > b.db.P || (int)pb.insns.size() > b.insn_cap || (int)pb.consts.size() > b.const_cap)
         return 1;
@@ -130,13 +131,14 @@ int stage(Bucket &b, const FvGpuIndex *g, int nq, const float *queries, const Pr
         memcpy(h + b.db.off_insns, pb.insns.data(), pb.insns.size() * sizeof(PredInsn));
     if (!pb.consts.empty())
         memcpy(h + b.db.off_consts, pb.consts.data(), pb.consts.size() * 8);
-    // lazy filters (tensor-core buckets whose programs are all in range
-    // form): no bitmaps, the scan tests a query's filter only on rows that
+    // lazy filters (tensor-core buckets whose programs are all broad range
+    // forms): no bitmaps, the scan tests a query's filter only on rows that
     // beat its threshold, instead of one full bitmap per query
-    bool lazy = b.mode == PV_MODE_LOW;
+    bool lazy = b.mode == PV_MODE_LOW && owner != nullptr;
     for (int p = 0; p < P && lazy; p++) {
         const PredProg &pp = pb.progs[p];
-        lazy = pp.ninsn == 1 && pb.insns[pp.insn0].kind == PV_NODE_RANGE;
+        lazy = prog_pass_estimate(owner, pb.insns.data() + pp.insn0, pp.ninsn,
+                                  pb.consts.data()) >= PV_LAZY_MIN_PASS;
     }
     int32_t *cnt = (int32_t *)(h + b.db.off_counts);
     cnt[0] = lazy ? 0 : P;
@@ -404,7 +406,7 @@ extern "C" int pv_stream_run(PvStream *s, int nq, const float *queries, const Fv
             b = c;
     s->last_fallback = 0;
     s->last_uncertain = 0;
-    if (!b || stage(*b, v, nq, queries, pb)) {
+    if (!b || stage(*b, v, nq, queries, pb, s->g)) {
         // predicates beyond the bucket's capacities: the index's own path
         s->last_fallback = 1;
         std::lock_guard<std::mutex> lg(s->g->mu);

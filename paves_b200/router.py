@@ -290,11 +290,12 @@ def label_actions(recall: np.ndarray, graph_ms: np.ndarray, scan_ms: float,
 
 def routed_batch(index, router: Optional[Router], queries: np.ndarray, preds, k, entries,
                  topb: Optional[int] = None, plan: Optional[np.ndarray] = None,
-                 margin: float = 0.0, bp: Optional[BatchPred] = None):
+                 margin: float = 0.0, bp: Optional[BatchPred] = None, split: bool = False):
     """pv_routed_batch -> (ids u64 [nq][topb], dists, cnt, decided ef per query,
-    executed (0 all scanned / 1 all graph / 2 mixed), stage_ms [3]: bitmaps, routing (beside the
+    executed (0 answered by the scan / 1 all graph / 2 split), stage_ms [3]: bitmaps, routing (beside the
     search), search; the batch took stage_ms[0] + stage_ms[2]). bp: the
-    batch's predicate arrays with entries, if already built."""
+    batch's predicate arrays with entries, if already built. split: each
+    query takes its own route even when the batch is scanned."""
     from .pred import concat
     L = _lib.lib()
     q = np.ascontiguousarray(queries, np.float32)
@@ -313,7 +314,8 @@ def routed_batch(index, router: Optional[Router], queries: np.ndarray, preds, k,
     rc = L.pv_routed_batch(index.handle, router._h if router is not None else None, nq, ptr(q),
                            ptr(bp.qd), ptr(bp.nodes), len(bp.nodes), ptr(bp.children),
                            len(bp.children), ptr(bp.invals), len(bp.invals), ptr(kk), topb,
-                           ptr(pl), margin, ptr(out), ptr(cnt), ptr(dec), C.byref(ex), ptr(st),
+                           ptr(pl), margin, int(split), ptr(out), ptr(cnt), ptr(dec), C.byref(ex),
+                           ptr(st),
                            err, len(err))
     if rc != 0:
         raise RuntimeError(err.value.decode())

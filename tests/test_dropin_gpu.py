@@ -72,7 +72,8 @@ def test_engine_graph_batch_runs_our_kernels(setup):
     gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
     for p in (datagen.graph_predicates()["sel10%"], None):
         hp = R.compile(p)
-        bp = R.serialize(hp)[0]
+        ser = R.serialize(hp)  # keeps the buffers the struct points into
+        bp = ser[0]
         for ef in (32, 128):
             ids, dists, cnt, exh = R.gpu_graph_batch(ds.queries, entries, [bp] * NQ, ef,
                                                      max(200000, 400 * ef))

@@ -70,7 +70,12 @@ def test_mixed_plan_scans_and_router_decisions(env):
     plan[5] = 0
     plan[11] = 0
     ids, dist, cnt, dec, ex, st = routed_batch(g, None, ds.queries, preds, k, ent, plan=plan)
-    assert ex == 2  # mixed: each query takes its own route
+    assert ex == 0  # a scanned batch answers every query from the scan
+    bi, bd, bc, _ = g.brute_batch(ds.queries, preds, 10)
+    assert np.array_equal(ids, bi) and np.array_equal(dist, bd)
+    ids, dist, cnt, dec, ex, st = routed_batch(g, None, ds.queries, preds, k, ent, plan=plan,
+                                               split=True)
+    assert ex == 2  # split: each query takes its own route
     bi, bd, bc, _ = g.brute_batch(ds.queries, preds, 10)
     sc = plan == 0
     assert np.array_equal(ids[sc], bi[sc]) and np.array_equal(dist[sc], bd[sc])
@@ -93,5 +98,5 @@ def test_mixed_plan_scans_and_router_decisions(env):
         a = r.decide(f, k, margin)
         want = np.where(a == 0, 0, np.maximum(np.array([0, 32, 64, 128, 256])[a], 10))
         assert np.array_equal(dec, want.astype(np.uint16))
-        assert ex == (1 if (want > 0).all() else 2 if (want > 0).any() else 0)
+        assert ex == (1 if (want > 0).all() else 0)
         assert (st >= 0).all()
