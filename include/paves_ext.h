@@ -315,6 +315,54 @@ int pv_stream_info(PvStream *s, int i, int *B, uint32_t *topb, int *mode, int *e
 int pv_stream_last(PvStream *s, int *uncertain, int *fallback);
 void pv_stream_free(PvStream *s);
 
+/* ---- persistent micro-batch kernel (no counterpart in the reference) ----
+ * The reference worker answers each micro-batch with separate synchronous
+ * launches (worker.c:268-276, loop worker.c:453-598). A PvServe keeps ONE
+ * cooperative kernel (one CTA per SM) resident on g's device, started from
+ * a captured CUDA graph when the runtime allows the capture (else launched
+ * directly), and feeds it a queue of staged micro-batches: uneven sizes
+ * (1..max_batch), a k per query (<= max_k) and a filter per query. Each
+ * batch runs inside the kernel as grid-synchronous phases (query prep,
+ * predicate bitmaps unless every filter is broad, seeding pass and merge,
+ * the tensor-core main pass, merge and exact re-rank) and its results are
+ * written into host-mapped memory. Every wait of the kernel is bounded by
+ * the GPU clock: the wait for the next batch by idle_ms (the kernel then
+ * leaves; the next pv_serve_run starts it again), each grid barrier by a
+ * limit after which the kernel leaves with a failure status (pv_serve_run
+ * returns -1 with "wait expired"), the scan's own waits as in the one-shot
+ * kernel. g must be a BF16 or FP8 upload and outlive the server; while the
+ * kernel is resident it holds every SM of the device, so other work on the
+ * device waits for it to leave (pv_serve_stop, or idle_ms without a batch).
+ * Batches beyond the capacities, and queries whose reduced-precision
+ * superset cannot be certified, run on g's ordinary path with the kernel
+ * stopped. out[nq][max_k] holds min(k, found) hits per query ascending by
+ * (dist, id); *device_ms the batch's time inside the kernel (GPU clock from
+ * taking the batch to its completion word). NULL / -1 + errbuf on error. */
+#define PV_SERVE_MAX_K 256
+typedef struct PvServe PvServe;
+PvServe *pv_serve_create(FvGpuIndex *g, int max_batch, uint32_t max_k, uint32_t idle_ms,
+                         char *errbuf, size_t errlen);
+int pv_serve_run(PvServe *s, int nq, const float *queries, const FvGpuQueryDesc *qd,
+                 const FvGpuPredNode *nodes, int nnodes, const int32_t *children, int nchildren,
+                 const double *invals, int ninvals, const uint32_t *k, FvHit *out,
+                 uint32_t *out_cnt, float *device_ms, char *errbuf, size_t errlen);
+/* running (the kernel is resident), last_exit of the last kernel (0 stopped
+ * or never started, 1 left after idle_ms without a batch, -1 a wait
+ * expired), batches completed, graph_launch (1: started from the captured
+ * graph), and for the last batch: fallback (ran on g's ordinary path),
+ * uncertain (queries re-run exactly). */
+int pv_serve_status(PvServe *s, int *running, int *last_exit, uint64_t *batches,
+                    int *graph_launch, int *fallback, int *uncertain);
+/* Stops the kernel (it leaves before its next batch) and waits for it. */
+int pv_serve_stop(PvServe *s, char *errbuf, size_t errlen);
+/* Limits for the next start: idle_ms, the grid-barrier limit barrier_ms,
+ * and skip_cta >= 0, which makes that CTA skip its arrival at the first
+ * barrier of the next batch (a failure made on the host side of the
+ * barrier protocol: the other CTAs' bounded waits expire; -1 none).
+ * Stops a resident kernel. -1 on bad values. */
+int pv_serve_limits(PvServe *s, uint32_t idle_ms, uint32_t barrier_ms, int skip_cta);
+void pv_serve_free(PvServe *s);
+
 /* Device time (ms) of the kernels of the last synchronous batch call on g. */
 float pv_last_kernel_ms(const FvGpuIndex *g);
 

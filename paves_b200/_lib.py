@@ -204,6 +204,16 @@ _EXT_SIGS["pv_tc_shape"] = (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c
 _EXT_SIGS["pv_tc_wide_superset"] = (C.c_int, [P, C.c_int])
 _EXT_SIGS["pv_hnsw_build_gpu"] = (P, [P, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_char_p, C.c_size_t])
+PV_SERVE_MAX_K = 256
+_EXT_SIGS.update({
+    "pv_serve_create": (P, [P, C.c_int, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t]),
+    "pv_serve_run": (C.c_int, [P, C.c_int, P, P, P, C.c_int, P, C.c_int, P, C.c_int, P, P, P, P,
+                               C.c_char_p, C.c_size_t]),
+    "pv_serve_status": (C.c_int, [P, P, P, P, P, P, P]),
+    "pv_serve_stop": (C.c_int, [P, C.c_char_p, C.c_size_t]),
+    "pv_serve_limits": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_int]),
+    "pv_serve_free": (None, [P]),
+})
 _EXT_SIGS["pv_tc_timeout"] = (C.c_int, [P, C.c_uint64])
 _EXT_SIGS["pv_filter_bound"] = (C.c_int, [P, P, C.c_int, P, C.c_int, P, C.c_int, P, C.c_char_p,
                                           C.c_size_t])
