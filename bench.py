@@ -860,11 +860,13 @@ def main():
     dev_ms, launches, graph_steps, mixed_steps = 0.0, 0, 0, 0
     st_sum = np.zeros(3)
     results = {}
+    cls_ms = {}
     t0 = time.perf_counter()
     for i in range(args.steps):
         c = i % nclass
         ids, dists, cnt, dec, ex, st = routed(c)
         dev_ms += float(st[0] + st[2])  # routing runs beside the search
+        cls_ms.setdefault(c, []).append(float(st[0] + st[2]))
         st_sum += st
         launches += int(L.pv_last_launches(gi.handle))
         graph_steps += int(ex == 1)
@@ -886,6 +888,7 @@ def main():
         r = [np.isin(xi[i, :xc[i]], ids[i, :cnt[i]]).sum() / max(1, int(xc[i]))
              for i in range(BATCH)]
         recall[name] = {"recall_at_10": round(float(np.mean(r)), 4),
+                        "ms": round(float(np.mean(cls_ms[c])), 4),
                         "path": {0: "bf16-scan", 1: "graph", 2: "mixed"}[int(ex)],
                         "graph_queries": int((dec > 0).sum())}
 

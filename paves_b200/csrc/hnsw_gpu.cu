@@ -2,7 +2,7 @@
 //
 // No counterpart in the reference: its builder is a CPU thread pool that
 // inserts rows one at a time (engine.cpp:698-1032). Here rows are inserted
-// in batches of doubling size (2048, then as many as are already in), and
+// in batches of doubling size (64, then as many as are already in), and
 // each batch takes exact candidates instead of insertion-time beam searches:
 //   1. candidates: each new node's C nearest nodes among all nodes inserted
 //      so far (its own batch included), exact, from this library's scans
@@ -339,7 +339,9 @@ int build_level(FvGpuIndex *g, int R, int C, uint32_t *d_lists, char *errbuf, si
     const int dpad = g->dpad;
     const int NVn = (dpad + 127) / 128;
     const int B = 2048;          // scan batch (queries per call)
-    const uint64_t first = 2048;  // first insertion batch
+    // first insertion batch: a few rows spread over the whole data set, so
+    // the earliest lists link distant regions (then doubling batches)
+    const uint64_t first = 64;
     cudaStream_t st = g->stream;
     // the rows' tensor map covers all rows, whatever prefix is scanned
     if (g->precision != FV_GPU_PREC_FP32 && !g->tmap_x_ok) {
@@ -523,7 +525,8 @@ extern "C" PvHnsw *pv_hnsw_build_gpu(const float *vectors, uint64_t count, int d
                                             device, precision, errbuf, errlen);
         if (!g) return fail();
         const int R = M;
-        const int C = (int)std::min<uint64_t>((uint64_t)candidates, n - 1);
+        // upper levels are small: twice the candidates (exact FP32 scans)
+        const int C = (int)std::min<uint64_t>((uint64_t)std::min(2 * candidates + 1, 1023), n - 1);
         std::vector<uint32_t> lists(n * (R + 1));
         uint32_t *d_lists = nullptr;
         int rc = 0;

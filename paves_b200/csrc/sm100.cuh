@@ -56,7 +56,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
                                           volatile int *abort) {
     for (uint32_t i = 0;; i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 63) == 63) {
+        if ((i & 63) == 0) {  // the first failed poll, then every 64th
             if (*abort) return false;
             if (globaltimer() > deadline) return false;
         }

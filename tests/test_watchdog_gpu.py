@@ -4,7 +4,7 @@ Every wait of scan_tc_kernel (TMA stages, MMA completion, tensor-memory
 buffers, the norm ring) gives up at a deadline; the kernel then records
 which role gave up, waits (with its own, separate 2 s limit) for the copies
 and MMAs it already issued, frees its tensor memory and returns. Here the
-limit is set to 1 us, so the first waits expire: the batch call must return
+limit is set to 1 ns, so the first wait that is not already over expires: the batch call must return
 -1 with the error message, nothing may fault or hang, and with the default
 limit restored the same index must answer a batch exactly (oracle)."""
 import numpy as np
@@ -22,7 +22,7 @@ def test_expired_waits_return_an_error_and_the_index_still_serves():
     L = _lib.lib()
     preds = [list(datagen.six_predicates().values())[2 + q % 4] for q in range(64)]
     gi.brute_batch(ds.queries, preds, 10)  # warm: scratch sized, kernels loaded
-    assert L.pv_tc_timeout(gi.handle, 1000) == 0  # 1 us
+    assert L.pv_tc_timeout(gi.handle, 1) == 0  # 1 ns: every wait that must wait expires
     for _ in range(3):
         with pytest.raises(GpuError, match="wait expired"):
             gi.brute_batch(ds.queries, preds, 10)
