@@ -12,7 +12,9 @@ filtered L2 top-10. A step is one batch; steps rotate through the classes.
             re-rank, or to the graph search at a per-query beam width
             (pv_routed_batch); queries/s over the device time of K steps
             (bitmaps, routing, search), max over ranks
-  plain_gpu the exact FP32 scan of the same batches (prepared, resident)
+  plain_gpu exact FP32 answers for the same batches (prepared, resident):
+            the f32 rows read as TF32 on the tensor cores with a certified
+            exact re-rank, and (cuda_cores_only) the CUDA-core scan
   e2e       the chosen path through the C ABI with host buffers: predicate
             compile + H2D + kernels + D2H, wall clock
   roofline  the tensor-core scan kernel: algorithmic bytes (rows once per
@@ -30,6 +32,12 @@ filtered L2 top-10. A step is one batch; steps rotate through the classes.
             fp32 and sq8, through the engine's batch call with host buffers
             (a subprocess): e2e queries/s, its profiler's kernel time, and
             its answers against the reference CPU's
+  graph_search_points  the graph search alone on the same index's graph:
+            filters at 1 %, 10 %, 50 %, ef 32..256, recall@10 and queries/s
+  uneven_microbatches  100 micro-batches over 10M x 96 FP8 rows (sizes
+            1..512, per-query k and filter) through the CUDA-graph executor
+            and through the persistent kernel: p50/p99 latency, queries/s
+  (--no-extras skips the last two)
 
 --impl reference times that reference CPU path alone (rank 0).
 Multi-GPU (torchrun): each rank serves its own batches on its own GPU
@@ -293,6 +301,8 @@ KERNEL_CASES = {
     # name: (batch, precision, mode, predicate kind index or None for rotation)
     "exact_b1": (1, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, 5),
     "exact_b64": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, None),
+    # the same on the CUDA cores alone (pv_exact_tc off)
+    "exact_b64_cuda": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, None),
     "bf16_b64": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, None),
     "fp8_b64": (64, _lib.FV_GPU_PREC_FP8, _lib.PV_MODE_LOW, None),
     # graph: 200k x 128 rows, HNSW M=16 efC=100, 64 queries, 10% filter, ef 64
@@ -325,6 +335,8 @@ def kernel_case(name, iters, tc_shape=None):
     else:
         preds = [classes[q % len(classes)][1] for q in range(nq)]
     gi = GpuIndex(ds.vectors, ds.cols, precision=prec)
+    if name.endswith("_cuda"):
+        _lib.lib().pv_exact_tc(gi.handle, 0)
     if tc_shape:
         if _lib.lib().pv_tc_shape(gi.handle, *tc_shape) != 0:
             raise ValueError(f"bad tensor-core shape {tc_shape}")
@@ -363,6 +375,28 @@ def stream_bench(args):
     wall time of the call; device time = the graph's CUDA-event time, or
     the persistent kernel's GPU-clock time from taking the batch to its
     completion word."""
+    res = stream_results(args.steps, args.warmup)
+    line = {
+        "metric": "uneven micro-batch QPS, 10M x 96 L2, FP8 + FP32 re-rank",
+        "value": res["graphs"]["value"], "unit": "queries/s", "n_gpus": 1,
+        "steps": args.steps, "higher_is_better": True, "dtype": "fp8-e4m3", "data": "synthetic",
+        "config": STREAM_CONFIG,
+    }
+    line.update({k: v for k, v in res["graphs"].items() if k != "value"})
+    line["persistent_kernel"] = res["persistent_kernel"]
+    print(json.dumps(line), flush=True)
+
+
+STREAM_CONFIG = {"workload": "10M x 96 Gaussian-mixture rows (256 components); micro-batch "
+                             "sizes log-uniform 1..512; k in {1, 10, 100} and a filter "
+                             "(selectivity log-uniform 0.05%-90%) per query",
+                 "rows": 10_000_000, "dim": 96, "max_batch": 512, "max_k": 100,
+                 "executor": "CUDA graph per batch-size bucket (value); persistent kernel "
+                             "beside it"}
+
+
+def stream_results(nsteps, nwarm):
+    """The measurement behind stream_bench: {"graphs": ..., "persistent_kernel": ...}."""
     from paves_b200.stream import Serve, Stream
     n, d = 10_000_000, 96
     ds = datagen.make_dataset(n, d, nq=1024, ncomp=256)
@@ -376,10 +410,10 @@ def stream_bench(args):
         k = rng.choice(np.array([1, 10, 100], np.uint32), nq)
         return ds.queries[idx], [stream_filter(rng) for _ in range(nq)], k
 
-    warm = [batch() for _ in range(max(3, args.warmup))]
-    steps = [batch() for _ in range(args.steps)]
+    warm = [batch() for _ in range(max(3, nwarm))]
+    steps = [batch() for _ in range(nsteps)]
     truth = {}
-    for i in range(0, args.steps, 10):  # the exact FP32 scan of every 10th batch
+    for i in range(0, nsteps, 10):  # the exact FP32 scan of every 10th batch
         q, preds, k = steps[i]
         bx = prepared_batch(gi, q, pred.concat(preds, n), 100, _lib.PV_MODE_EXACT)
         batch_run(bx, 1)
@@ -431,41 +465,16 @@ def stream_bench(args):
         sv.close()
     except Exception as e:  # reported, the graph executor's line stands
         persistent = {"failed": str(e)}
-    line = {
-        "metric": "uneven micro-batch QPS, 10M x 96 L2, FP8 + FP32 re-rank",
-        "value": graphs["value"], "unit": "queries/s", "n_gpus": 1,
-        "steps": args.steps, "higher_is_better": True, "dtype": "fp8-e4m3", "data": "synthetic",
-        "config": {"workload": "10M x 96 Gaussian-mixture rows (256 components); micro-batch "
-                               "sizes log-uniform 1..512; k in {1, 10, 100} and a filter "
-                               "(selectivity log-uniform 0.05%-90%) per query",
-                   "rows": n, "dim": d, "max_batch": 512, "max_k": 100,
-                   "executor": "CUDA graph per batch-size bucket (value); persistent kernel "
-                               "beside it"},
-    }
-    line.update({k: v for k, v in graphs.items() if k != "value"})
-    line["persistent_kernel"] = persistent
-    print(json.dumps(line), flush=True)
     gi.close()
+    return {"graphs": graphs, "persistent_kernel": persistent}
 
 
-def graph_bench(args):
-    """Filtered graph search: the 1M x 128 set, HNSW (M=16, efConstruction
-    200) built by the library, 64 queries per batch, filters at 1%, 10% and
-    50%, ef in {32, 64, 128, 256}; recall@10 against the exact scan and
-    device-time and wall-clock (host buffers) QPS, beside the reference
-    engine's HnswCursor (built from its sources) on the same graph file, one
-    query per host thread, and the reference's own GPU graph kernel through
-    the engine's batch call (wall clock, host buffers)."""
-    from concurrent.futures import ThreadPoolExecutor
-    ds, _, _ = make_workload()
-    cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
-    t0 = time.perf_counter()
-    h = shared_graph(ds.vectors, 0, None, cache)
-    build_s = time.perf_counter() - t0
-    gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
+def graph_points(gi, q, ent, steps, warmup):
+    """Config 3's points on gi's graph: filters at 1 %, 10 % and 50 %, ef 32 to
+    256, 64-query batches; recall@10 against the exact scan, device-time
+    and wall-clock queries/s, mean steps and visited nodes per query."""
     L = _lib.lib()
-    q = ds.queries[:BATCH]
-    ent = h.entries(q)
+    args = argparse.Namespace(steps=steps, warmup=warmup)
     res = []
     for name, p in datagen.graph_predicates().items():
         preds = [p] * BATCH
@@ -490,6 +499,28 @@ def graph_bench(args):
                         "qps_e2e": round(BATCH * reps / wall, 1),
                         "mean_steps": round(float(st[:, 0].mean()), 1),
                         "mean_visited": round(float(st[:, 1].mean()), 1)})
+    return res
+
+
+def graph_bench(args):
+    """Filtered graph search: the 1M x 128 set, HNSW (M=16, efConstruction
+    200) built by the library, 64 queries per batch, filters at 1%, 10% and
+    50%, ef in {32, 64, 128, 256}; recall@10 against the exact scan and
+    device-time and wall-clock (host buffers) QPS, beside the reference
+    engine's HnswCursor (built from its sources) on the same graph file, one
+    query per host thread, and the reference's own GPU graph kernel through
+    the engine's batch call (wall clock, host buffers)."""
+    from concurrent.futures import ThreadPoolExecutor
+    ds, _, _ = make_workload()
+    cache = os.path.join(tempfile.gettempdir(), f"paves_bench_hnsw_{N_ROWS}x{DIM}.npz")
+    t0 = time.perf_counter()
+    h = shared_graph(ds.vectors, 0, None, cache)
+    build_s = time.perf_counter() - t0
+    gi = GpuIndex(ds.vectors, ds.cols, l0=h.l0)
+    L = _lib.lib()
+    q = ds.queries[:BATCH]
+    ent = h.entries(q)
+    res = graph_points(gi, q, ent, args.steps, args.warmup)
     # the same searches on the graph the GPU builder makes (pv_hnsw_build_gpu)
     gpu_built = {}
     try:
@@ -756,6 +787,9 @@ def main():
                     help="skip the baseline legs (reference CPU, reference GPU, parity)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference GPU leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the graph points (1M x 128 at ef 32..256) and the uneven "
+                         "micro-batch stream (10M x 96) reported beside the headline")
     ap.add_argument("--workload", default="headline",
                     choices=["headline", "stream", "graph", "batches"],
                     help="stream: uneven micro-batches over 10M x 96 FP8 (p50/p99 latency); "
@@ -827,19 +861,31 @@ def main():
         bp = pred.concat([p] * BATCH, N_ROWS, entries=ent)
         cls.append((name, p, q, ent, bp))
 
-    # plain path: exact FP32 scan of each class batch (prepared, resident)
-    plain = []
-    for name, p, q, ent, bp in cls:
-        bx = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_EXACT)
-        batch_run(bx, 3)
-        plain.append(bx)
+    # plain path: exact FP32 scan of each class batch (prepared, resident):
+    # on the tensor cores (f32 rows read as TF32, certified exact), and on
+    # the CUDA cores alone (pv_exact_tc off)
     per_class = max(1, args.steps // nclass)
-    plain_ms = 0.0
-    for bx in plain:
-        ms, _ = batch_run(bx, per_class)
-        plain_ms += ms
-    plain_qps = BATCH * per_class * nclass / (plain_ms / 1e3)
-    exact = [fetch(bx, BATCH, TOPK) for bx in plain]
+
+    def plain_leg():
+        bxs, ms_tot, on_tc = [], 0.0, 0
+        for name, p, q, ent, bp in cls:
+            bx = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_EXACT)
+            batch_run(bx, 3)
+            ms, _ = batch_run(bx, per_class)
+            ms_tot += ms
+            on_tc += L.pv_last_exact_tc(gi.handle)
+            bxs.append(bx)
+        ans = [fetch(bx, BATCH, TOPK) for bx in bxs]
+        for bx in bxs:
+            L.pv_batch_free(bx)
+        return BATCH * per_class * nclass / (ms_tot / 1e3), ans, on_tc
+
+    plain_qps, exact, plain_tc = plain_leg()
+    L.pv_exact_tc(gi.handle, 0)
+    simt_qps, exact_simt, _ = plain_leg()
+    L.pv_exact_tc(gi.handle, 1)
+    simt_same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                    for a, b in zip(exact, exact_simt))
 
     def routed(c):
         name, p, q, ent, bp = cls[c]
@@ -953,8 +999,18 @@ def main():
             cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"failed: {e}"}
 
-    for bx in plain:
-        L.pv_batch_free(bx)
+    extras = rank == 0 and world == 1 and not args.no_extras
+    graph_pts, stream_res = None, None
+    if extras:  # the graph search alone on this index's graph (64 queries per point)
+        qg = np.ascontiguousarray(ds.queries[:BATCH], np.float32)
+        graph_pts = graph_points(gi, qg, hnsw.entries(qg), min(args.steps, 10), 1)
+    router.close()
+    gi.close()
+    if extras:
+        try:
+            stream_res = stream_results(100, 5)
+        except Exception as e:  # informative; the headline stands
+            stream_res = {"failed": str(e)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
@@ -978,7 +1034,12 @@ def main():
                                 "routing_beside_search": round(st_sum[1] / args.steps, 4),
                                 "search": round(st_sum[2] / args.steps, 4)},
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
-                          "path": "exact FP32 scan"},
+                          "path": "exact FP32 results: f32 rows read as TF32 on the tensor "
+                                  "cores, certified exact (the sparse route for selective "
+                                  "filters)",
+                          "tensor_core_batches": f"{plain_tc} of {nclass}",
+                          "cuda_cores_only": round(simt_qps, 1),
+                          "same_answers_as_cuda_cores": simt_same},
             "scan_only": {"value": round(scan_only_qps, 1), "unit": "queries/s",
                           "path": "bf16 scan + re-rank (sparse route for selective "
                                   "filters), no router", "classes": per_cls},
@@ -1001,10 +1062,12 @@ def main():
             "cpu_baseline": cpu,
             "parity_vs_reference_cpu": parity,
             "reference_gpu": ref_gpu,
+            "graph_search_points": graph_pts,
+            "uneven_microbatches": None if stream_res is None else {
+                "config": STREAM_CONFIG, "unit": "queries/s", "dtype": "fp8-e4m3",
+                **stream_res},
         }
         print(json.dumps(line), flush=True)
-    router.close()
-    gi.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -425,6 +425,16 @@ int pv_tc_wide_superset(FvGpuIndex *g, int on);
  * frees its tensor memory and returns, and the batch call returns -1 with
  * "wait expired" in errbuf; the index stays usable. -1: bad value. */
 int pv_tc_timeout(FvGpuIndex *g, uint64_t ns);
+/* Exact-mode batches (FP32 uploads through fv_gpu_brute_batch, or
+ * PV_MODE_EXACT) of 16+ queries over rows of at most 128 dims scan on the
+ * tensor cores: the f32 rows read as TF32, the top 4 x topb (at least 16;
+ * topb itself on integer rows, where the distances are exact) re-ranked in
+ * FP32, and each query's answer certified by an error bound of the scan
+ * distances; a query the bound cannot separate is re-run on the CUDA-core
+ * scan. on = 0 keeps every exact batch on the CUDA cores. -1: bad value.
+ * pv_last_exact_tc: 1 if the last brute batch on g took the tensor cores. */
+int pv_exact_tc(FvGpuIndex *g, int on);
+int pv_last_exact_tc(const FvGpuIndex *g);
 int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                     const int32_t *children, int nchildren, const double *invals, int ninvals,
                     uint64_t *bound, char *errbuf, size_t errlen);

@@ -202,6 +202,8 @@ _EXT_SIGS["pv_index_upload_prepared"] = (P, [P, P, P, P, C.c_uint32, C.c_uint64,
 PV_PART_LOWP_ROWS, PV_PART_NORMS, PV_PART_SCALES = 1, 2, 3
 _EXT_SIGS["pv_tc_shape"] = (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int])
 _EXT_SIGS["pv_tc_wide_superset"] = (C.c_int, [P, C.c_int])
+_EXT_SIGS["pv_exact_tc"] = (C.c_int, [P, C.c_int])
+_EXT_SIGS["pv_last_exact_tc"] = (C.c_int, [P])
 _EXT_SIGS["pv_hnsw_build_gpu"] = (P, [P, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_char_p, C.c_size_t])
 PV_SERVE_MAX_K = 256

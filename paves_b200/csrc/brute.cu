@@ -121,6 +121,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
     g->last_sparse = 0;
+    g->last_exact_tc = 0;
     if (db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024) {
         g->tc_err = nullptr;
         g->tc_unc = nullptr;
@@ -144,6 +145,18 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
                            errbuf, errlen, db.counts_on_device ? &lz : nullptr))
             return -1;
+        if (ev) cudaEventRecord(ev[4], g->stream);
+        return 0;
+    }
+    if (mode == PV_MODE_EXACT && nq >= PV_EXACT_TC_MIN_NQ && tf32_supported(g) &&
+        tf32_superset(g, topb, db.q_amax) > 0) {
+        TcLazy lz{(const int *)(d + db.off_counts) + 3, d_progs, d_insns, d_consts,
+                  db.nconsts};
+        if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
+                           s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
+                           errbuf, errlen, db.counts_on_device ? &lz : nullptr, true))
+            return -1;
+        g->last_exact_tc = 1;
         if (ev) cudaEventRecord(ev[4], g->stream);
         return 0;
     }
@@ -277,12 +290,13 @@ int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &p
     std::vector<FvHit> so((size_t)n * topb);
     std::vector<uint32_t> sc(n);
     std::vector<uint8_t> st(n);
-    const int launches = g->launches, nunc = n;
-    if (brute_run_host(g, n, sq.data(), sub, topb, PV_MODE_EXACT, so.data(), sc.data(),
+    const int launches = g->launches, nunc = n, took_tc = g->last_exact_tc;
+    if (brute_run_host(g, n, sq.data(), sub, topb, PV_MODE_SIMT, so.data(), sc.data(),
                        st.data(), errbuf, errlen))
         return -1;
     g->launches += launches;
     g->last_uncertain = nunc;
+    g->last_exact_tc = took_tc;  // the batch's own route
     for (int i = 0; i < n; i++) {
         const int q = idx[i];
         memcpy(out + (size_t)q * topb, &so[(size_t)i * topb], sizeof(FvHit) * sc[i]);

@@ -218,6 +218,15 @@ extern "C" int pv_tc_wide_superset(FvGpuIndex *g, int on) {
     return 0;
 }
 
+extern "C" int pv_exact_tc(FvGpuIndex *g, int on) {
+    if (!g || on < 0 || on > 1) return -1;
+    std::lock_guard<std::mutex> lk(g->mu);
+    g->exact_tc = on;
+    return 0;
+}
+
+extern "C" int pv_last_exact_tc(const FvGpuIndex *g) { return g ? g->last_exact_tc : 0; }
+
 extern "C" int pv_filter_bound(const FvGpuIndex *g, const FvGpuPredNode *nodes, int nnodes,
                                const int32_t *children, int nchildren, const double *invals,
                                int ninvals, uint64_t *bound, char *errbuf, size_t errlen) {

@@ -346,7 +346,8 @@ int build_level(FvGpuIndex *g, int R, int C, uint32_t *d_lists, char *errbuf, si
     // the rows' tensor map covers all rows, whatever prefix is scanned
     if (g->precision != FV_GPU_PREC_FP32 && !g->tmap_x_ok) {
         CUtensorMap m;
-        if (!tc_make_tmap(&m, g->d_vlow, g->precision == FV_GPU_PREC_FP8, (uint64_t)g->kpad,
+        if (!tc_make_tmap(&m, g->d_vlow, g->precision == FV_GPU_PREC_FP8 ? TCK_FP8 : TCK_BF16,
+                          (uint64_t)g->kpad,
                           g->count)) {
             snprintf(errbuf, errlen, "hnsw gpu: tensor map encoding failed");
             return -1;

@@ -49,6 +49,25 @@ __global__ void to_bf16_kernel(const float *__restrict__ src, int dpad, int dim,
     if (lane == 0) norm[row] = acc;
 }
 
+// ||x||^2 of the f32 rows (one warp per row) and their maximum (the bits
+// of non-negative floats order like the floats)
+__global__ void norm32_kernel(const float *__restrict__ src, int dpad, uint64_t nrows,
+                              float *__restrict__ norm, unsigned *__restrict__ nmax) {
+    const int lane = threadIdx.x & 31;
+    uint64_t row = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (row >= nrows) return;
+    float acc = 0.f;
+    for (int j = lane; j < dpad; j += 32) {
+        const float v = src[row * dpad + j];
+        acc = fmaf(v, v, acc);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        norm[row] = acc;
+        atomicMax(nmax, __float_as_uint(acc));
+    }
+}
+
 // fp32 rows -> fp8-e4m3 rows with one scale per row (absmax / 448), plus
 // the squared norm of the dequantized row.
 __global__ void to_fp8_kernel(const float *__restrict__ src, int dpad, int dim,
@@ -198,6 +217,7 @@ extern "C" void fv_gpu_index_free(FvGpuIndex *g) {
         cudaFree(g->d_vlow);
         cudaFree(g->d_vscale);
         cudaFree(g->d_norm);
+        cudaFree(g->d_norm32);
     }
     Buf *bufs[] = {&g->scan.stage_h, &g->scan.stage_d, &g->scan.bitmaps, &g->scan.popcnt,
                    &g->scan.tau, &g->scan.part, &g->scan.part_cnt, &g->scan.cand,
@@ -329,6 +349,26 @@ FvGpuIndex *upload_impl(const float *vectors, const double *cols, const uint32_t
 
     // the BF16 exactness certificate's input: scanned here, or stored
     g->row_amax = prep ? prep->row_amax : pv_integral_amax(vectors, count * (uint64_t)dim);
+
+    // f32 row norms for the exact mode's tensor-core scan (padded to whole
+    // 128-row tiles, then the maximum's word)
+    {
+        const size_t rows_pad32 = (size_t)((count + 127) / 128) * 128;
+        if ((e = cudaMalloc(&g->d_norm32, rows_pad32 * 4 + 16)) != cudaSuccess)
+            return bail("f32 norms", e);
+        unsigned *d_max = (unsigned *)(g->d_norm32 + rows_pad32);
+        unsigned h_max = 0;
+        if ((e = cudaMemsetAsync(g->d_norm32, 0, rows_pad32 * 4 + 16, g->stream)) != cudaSuccess)
+            return bail("f32 norms", e);
+        norm32_kernel<<<(unsigned)((count + 7) / 8), 256, 0, g->stream>>>(g->d_vecs, dpad, count,
+                                                                         g->d_norm32, d_max);
+        if ((e = cudaGetLastError()) != cudaSuccess) return bail("f32 norms", e);
+        if ((e = cudaMemcpyAsync(&h_max, d_max, 4, cudaMemcpyDeviceToHost, g->stream)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(g->stream)) != cudaSuccess)
+            return bail("f32 norms", e);
+        memcpy(&g->norm32_max, &h_max, 4);
+    }
 
     if (precision != FV_GPU_PREC_FP32) {
         const bool f8 = precision == FV_GPU_PREC_FP8;
@@ -465,6 +505,9 @@ FvGpuIndex *index_view(const FvGpuIndex *g) {
     v->d_vlow = g->d_vlow;
     v->d_vscale = g->d_vscale;
     v->d_norm = g->d_norm;
+    v->d_norm32 = g->d_norm32;
+    v->norm32_max = g->norm32_max;
+    v->exact_tc = g->exact_tc;
     v->row_amax = g->row_amax;
     v->sorted_cols = g->sorted_cols;
     v->sm_count = g->sm_count;

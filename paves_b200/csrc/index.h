@@ -99,6 +99,11 @@ struct FvGpuIndex {
     float *d_vscale = nullptr;  // fp8 per-row scale
     float *d_norm = nullptr;    // ||x||^2 of the stored low-precision row
     float row_amax = -1.f;      // max |x| if all rows are integers <= 256, else -1
+    // the exact mode's tensor-core scan (f32 rows read as TF32)
+    float *d_norm32 = nullptr;  // [rows padded to 128] ||x||^2 of the f32 rows
+    float norm32_max = 0.f;     // largest of them
+    int exact_tc = 1;           // exact-mode batches may take it (0: CUDA cores only)
+    int last_exact_tc = 0;      // the last brute batch took it
 
     int sm_count = 0;
     cudaStream_t stream = nullptr;
@@ -123,9 +128,13 @@ struct FvGpuIndex {
     // when their buffer or row count changes)
     alignas(64) unsigned char tmap_x[128] = {};
     alignas(64) unsigned char tmap_q[128] = {};
+    alignas(64) unsigned char tmap_x32[128] = {};  // the f32 rows (exact mode)
     bool tmap_x_ok = false;
+    bool tmap_x32_ok = false;
+    uint64_t tmap_x32_rows = 0;
     const void *tmap_q_ptr = nullptr;
     uint64_t tmap_q_rows = 0;
+    int tmap_q_kind = -1;
     bool view = false;  // shares another handle's device data, owns only scratch
     int last_superset = 0;  // candidates re-ranked per query by the last TC scan
     float last_kernel_ms = 0.f;  // device time of the last batch's kernels

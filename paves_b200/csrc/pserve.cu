@@ -207,7 +207,7 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
         {
             const int rows = pl.nqpad;
             for (int qi = blockIdx.x * NW + warp; qi < rows; qi += G * NW)
-                query_prep_row(qi, lane, qf, pl.nq, p.dpad, p.dim, pl.bq, p.kpad, FP8, qb,
+                query_prep_row(qi, lane, qf, pl.nq, p.dpad, p.dim, pl.bq, p.kpad, FP8 ? TCK_FP8 : TCK_BF16, qb,
                                p.qnorm, FP8 ? p.qscale : nullptr, p.tau, p.dcnt,
                                pl.certify ? p.fullmin : nullptr, p.err);
             for (int i = blockIdx.x * NT + tid; i < pl.P; i += G * NT) p.popcnt[i] = 0;
@@ -273,7 +273,7 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
             // shared memory the merges wrote is refilled by TMA (async proxy)
             fence_proxy_async();
             __syncthreads();
-            if (scans && !tc_pass<FP8, EPI>(&tmX, &p.tmQ[slot], sa, sm, s_tmem, run, &s_abort,
+            if (scans && !tc_pass<FP8 ? TCK_FP8 : TCK_BF16, EPI>(&tmX, &p.tmQ[slot], sa, sm, s_tmem, run, &s_abort,
                                             qtile, rgrp)) {
                 failed = true;
                 break;
@@ -302,7 +302,7 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
         a.fullmin = pl.certify ? p.fullmin : nullptr;
         fence_proxy_async();
         __syncthreads();
-        if (scans && !tc_pass<FP8, EPI>(&tmX, &p.tmQ[slot], a, sm, s_tmem, run, &s_abort, qtile,
+        if (scans && !tc_pass<FP8 ? TCK_FP8 : TCK_BF16, EPI>(&tmX, &p.tmQ[slot], a, sm, s_tmem, run, &s_abort, qtile,
                                         rgrp)) {
             failed = true;
             break;
@@ -526,7 +526,7 @@ extern "C" PvServe *pv_serve_create(FvGpuIndex *g, int max_batch, uint32_t max_k
     // row tensor map (the index's own)
     if (!g->tmap_x_ok) {
         CUtensorMap m;
-        if (!tc_make_tmap(&m, g->d_vlow, fp8, (uint64_t)g->kpad, g->count))
+        if (!tc_make_tmap(&m, g->d_vlow, fp8 ? TCK_FP8 : TCK_BF16, (uint64_t)g->kpad, g->count))
             return fail("tensor map", cudaSuccess);
         memcpy(g->tmap_x, &m, sizeof(m));
         g->tmap_x_ok = true;
@@ -551,7 +551,8 @@ extern "C" PvServe *pv_serve_create(FvGpuIndex *g, int max_batch, uint32_t max_k
     {
         std::vector<CUtensorMap> maps(SV_SLOTS);
         for (int i = 0; i < SV_SLOTS; i++)
-            if (!tc_make_tmap(&maps[i], s->qbuf.as<unsigned char>() + i * a.qbuf_bytes, fp8,
+            if (!tc_make_tmap(&maps[i], s->qbuf.as<unsigned char>() + i * a.qbuf_bytes,
+                              fp8 ? TCK_FP8 : TCK_BF16,
                               (uint64_t)g->kpad, (uint64_t)nqpad))
                 return fail("tensor map", cudaSuccess);
         if ((e = s->tmq.ensure(sizeof(CUtensorMap) * SV_SLOTS)) != cudaSuccess ||
@@ -794,8 +795,11 @@ extern "C" int pv_serve_run(PvServe *s, int nq, const float *queries, const FvGp
     for (;;) {
         if (done[slot] >= seq) break;
         if (!sv_alive(s)) {
-            if (s->running && sv_reap(s, errbuf, errlen)) return -1;
-            if (s->last_exit < 0) {
+            // a kernel that left with a failure while this batch waited (an
+            // earlier failure is history: the kernel is simply started again)
+            const bool reaped = s->running;
+            if (reaped && sv_reap(s, errbuf, errlen)) return -1;
+            if (reaped && s->last_exit < 0) {
                 snprintf(errbuf, errlen, "serve: a wait of the persistent kernel expired");
                 // the batch was not taken: rewind the queue, so a restarted
                 // kernel never takes this slot before its next batch lands

@@ -143,6 +143,15 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns);
 int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax);
 bool tc_supported(const FvGpuIndex *g);
+int tf32_superset(const FvGpuIndex *g, uint32_t topb, float q_amax);
+bool tf32_supported(const FvGpuIndex *g);
+// Exact-mode batches of at least this many queries scan on the tensor cores
+// (f32 rows read as TF32 + certified exact re-rank); smaller ones stream
+// the f32 rows through the CUDA cores, bandwidth-bound either way.
+constexpr int PV_EXACT_TC_MIN_NQ = 16;
+// internal brute mode: exact on the CUDA cores only (the re-run of queries
+// the tensor-core scan could not certify)
+constexpr int PV_MODE_SIMT = 2;
 // Lazy filters for the tensor-core scan: *flag (device memory, read when
 // the kernel runs) != 0 means the batch has no bitmaps and every program is
 // in range form; the scan then evaluates a query's program only for rows
@@ -159,7 +168,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen, const TcLazy *lz = nullptr);
+                   size_t errlen, const TcLazy *lz = nullptr, bool tf32 = false);
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);

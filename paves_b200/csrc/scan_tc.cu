@@ -45,7 +45,7 @@ namespace pv {
 
 using namespace sm100;
 
-template <bool FP8, int EPI>
+template <int KIND, int EPI>
 __global__ void __launch_bounds__(64 + 128 * EPI, 1)
 scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmQ,
                TcArgs a) {
@@ -67,7 +67,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     __syncthreads();
     tc_fence_after();
     TcRun run;
-    tc_pass<FP8, EPI>(&tmX, &tmQ, a, sm, s_tmem, run, &s_abort, blockIdx.x % a.qtiles,
+    tc_pass<KIND, EPI>(&tmX, &tmQ, a, sm, s_tmem, run, &s_abort, blockIdx.x % a.qtiles,
                       blockIdx.x / a.qtiles);
     if (warp == 1) {
         tc_fence_after();
@@ -86,14 +86,14 @@ namespace pv {
 // the scan's per-query state for query qi < nq: bound tau (none), dense run
 // count, full-list minimum (if tracked), and the watchdog word.
 __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad, int dim,
-                                  int nqpad, int bq, int kelems, bool fp8,
+                                  int nqpad, int bq, int kelems, int kind,
                                   unsigned char *__restrict__ out, float *__restrict__ qnorm,
                                   float *__restrict__ qscale, unsigned long long *__restrict__ tau,
                                   uint32_t *__restrict__ dcnt,
                                   unsigned long long *__restrict__ fullmin, int *__restrict__ err) {
     const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (qi >= nqpad) return;
-    query_prep_row(qi, threadIdx.x & 31, q, nq, dpad, dim, bq, kelems, fp8, out, qnorm, qscale,
+    query_prep_row(qi, threadIdx.x & 31, q, nq, dpad, dim, bq, kelems, kind, out, qnorm, qscale,
                    tau, dcnt, fullmin, err);
 }
 
@@ -108,10 +108,10 @@ rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict_
               uint32_t topb, const int32_t *__restrict__ qprog,
               const unsigned long long *__restrict__ popcnt, uint64_t nrows,
               FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
-              uint8_t *__restrict__ trunc) {
+              uint8_t *__restrict__ trunc, const RerankCert cert) {
     __shared__ uint64_t keys[TC_MAX_SUPERSET];
     rerank_query<256>(blockIdx.x, keys, vecs, dpad, queries, cand, cand_cnt, S, topb, qprog, popcnt,
-                 nrows, out, out_cnt, trunc);
+                      nrows, out, out_cnt, trunc, cert);
 }
 
 // ---------------------------------------------------------------- merge
@@ -191,17 +191,20 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // 2-D row-major [rows][inner] tensor map with 128-byte swizzled boxes of
-// [128 rows][128 bytes].
-bool tc_make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner, uint64_t rows) {
+// [128 rows][128 bytes] (elements of the operand kind: fp8, bf16 or f32).
+// Columns past `inner` read as zeros.
+bool tc_make_tmap(CUtensorMap *m, const void *ptr, int kind, uint64_t inner, uint64_t rows) {
     auto enc = get_encode();
     if (!enc) return false;
-    const uint32_t esz = fp8 ? 1 : 2;
+    const uint32_t esz = (uint32_t)tck_esz(kind);
     cuuint64_t dims[2] = {inner, rows};
     cuuint64_t strides[1] = {inner * esz};
     cuuint32_t box[2] = {TC_KB_BYTES / esz, TC_BN};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
-                     const_cast<void *>(ptr), dims, strides, box, estr,
+    const CUtensorMapDataType dt = kind == TCK_FP8    ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                   : kind == TCK_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                      : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    CUresult r = enc(m, dt, 2, const_cast<void *>(ptr), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -217,6 +220,24 @@ int tc_superset(const FvGpuIndex *g, uint32_t topb, float q_amax) {
                        pv_bf16_exact(g->dim, g->row_amax, q_amax);
     const int s = exact ? (int)topb : 4 * (int)topb;
     return s <= TC_MAX_SUPERSET ? s : 0;  // 0: topb beyond the superset capacity
+}
+
+// The exact scan on the tensor cores reads the f32 rows as TF32 and
+// re-ranks a superset exactly: S = k when the upload certified integer rows
+// (TF32 keeps integers up to 2048 exactly, so the norm-form distances are
+// exact as in the BF16 case), else 4k (at least 16), each query's answer
+// then certified by the re-rank's error bound (RerankCert) and re-run on the
+// CUDA cores when the bound does not separate it. 0 = topb too large.
+int tf32_superset(const FvGpuIndex *g, uint32_t topb, float q_amax) {
+    const bool exact = !g->force_wide_superset && pv_bf16_exact(g->dim, g->row_amax, q_amax);
+    const int s = exact ? (int)topb : std::max(4 * (int)topb, 16);
+    return s <= TC_MAX_SUPERSET ? s : 0;
+}
+
+// Rows of at most 128 f32 (the query tile stays 64 KB of shared memory),
+// at least 8 row tiles, and not switched off for the index.
+bool tf32_supported(const FvGpuIndex *g) {
+    return g->exact_tc && g->d_norm32 && g->dpad <= 128 && g->count >= 8 * (uint64_t)TC_BN;
 }
 
 bool tc_supported(const FvGpuIndex *g) {
@@ -238,38 +259,46 @@ bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
     return tc_smem(g->kpad * esz / TC_KB_BYTES, ns, KP, epi) <= 227 * 1024;
 }
 
-template <int EPI>
-static cudaError_t tc_launch(bool fp8, int grid, size_t smem, cudaStream_t st,
-                            const CUtensorMap &tmX, const CUtensorMap &tmQ, const TcArgs &a) {
-    const void *fn = fp8 ? (const void *)scan_tc_kernel<true, EPI>
-                         : (const void *)scan_tc_kernel<false, EPI>;
-    cudaError_t e = raise_smem_limit(fn, smem);
+template <int KIND, int EPI>
+static cudaError_t tc_launch_kind(int grid, size_t smem, cudaStream_t st, const CUtensorMap &tmX,
+                                  const CUtensorMap &tmQ, const TcArgs &a) {
+    cudaError_t e = raise_smem_limit((const void *)scan_tc_kernel<KIND, EPI>, smem);
     if (e != cudaSuccess) return e;
-    if (fp8)
-        scan_tc_kernel<true, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
-    else
-        scan_tc_kernel<false, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
+    scan_tc_kernel<KIND, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
     return cudaGetLastError();
+}
+
+template <int EPI>
+static cudaError_t tc_launch(int kind, int grid, size_t smem, cudaStream_t st,
+                            const CUtensorMap &tmX, const CUtensorMap &tmQ, const TcArgs &a) {
+    if (kind == TCK_FP8) return tc_launch_kind<TCK_FP8, EPI>(grid, smem, st, tmX, tmQ, a);
+    if (kind == TCK_TF32) return tc_launch_kind<TCK_TF32, EPI>(grid, smem, st, tmX, tmQ, a);
+    return tc_launch_kind<TCK_BF16, EPI>(grid, smem, st, tmX, tmQ, a);
 }
 
 // Launches query prep, the tensor-core scan, the per-query merge and the
 // exact re-rank. Inputs: f32 queries [nq][dpad] on the device, predicate
-// programs/bitmaps already built.
+// programs/bitmaps already built. tf32: scan the f32 rows themselves (the
+// exact mode), else the upload's BF16 / FP8 rows.
 int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen, const TcLazy *lz) {
-    const bool fp8 = g->precision == FV_GPU_PREC_FP8;
-    const int esz = fp8 ? 1 : 2;
-    const int kblocks = g->kpad * esz / TC_KB_BYTES;
-    const int S = tc_superset(g, topb, q_amax);
+                   size_t errlen, const TcLazy *lz, bool tf32) {
+    const bool fp8 = !tf32 && g->precision == FV_GPU_PREC_FP8;
+    const int kind = tf32 ? TCK_TF32 : fp8 ? TCK_FP8 : TCK_BF16;
+    const int esz = tck_esz(kind);
+    // elements of K per row: the low-precision row pitch, or dpad rounded up
+    // to whole 32-element boxes (the f32 rows' tail boxes read zeros)
+    const int kelems = tf32 ? ((g->dpad + 31) & ~31) : g->kpad;
+    const int kblocks = kelems * esz / TC_KB_BYTES;
+    const int S = tf32 ? tf32_superset(g, topb, q_amax) : tc_superset(g, topb, q_amax);
     const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
     g->last_superset = S;
     g->tc_unc = nullptr;
-    if (!S || !tc_supported(g)) {
-        snprintf(errbuf, errlen, "gpu: reduced-precision scan not available for this batch");
+    if (!S || !(tf32 ? tf32_supported(g) : tc_supported(g))) {
+        snprintf(errbuf, errlen, "gpu: tensor-core scan not available for this batch");
         return -1;
     }
     // two epilogue warp groups (each row half of a tile) when the lists fit,
@@ -312,7 +341,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     grow = (int)((ntiles_all + tpc - 1) / tpc);
 
     ScanScratch &s = g->scan;
-    const size_t qbytes = (size_t)nqpad * g->kpad * esz;
+    const size_t qbytes = (size_t)nqpad * kelems * esz;
     const size_t off_qn = (qbytes + 255) & ~(size_t)255;
     const size_t off_qs = off_qn + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
     const size_t off_err = off_qs + (((size_t)nqpad * 4 + 255) & ~(size_t)255);
@@ -334,27 +363,35 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     unsigned char *c = s.cand.as<unsigned char>();
     int *d_err = (int *)(c + off_err);
     const bool certify = KP < S;  // lists shorter than the superset
+    // inexact scan distances of exact-mode batches: the re-rank certifies
+    const bool num_cert = tf32 && S > (int)topb;
 
     g->launches += 4;  // query prep, main pass, merge, re-rank
     query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
-        d_q, nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, g->kpad, fp8, c, (float *)(c + off_qn),
-        fp8 ? (float *)(c + off_qs) : nullptr, s.tau.as<unsigned long long>(), d_dcnt,
-        certify ? d_fullmin : nullptr, d_err);
+        d_q, nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, kelems, kind, c,
+        (float *)(c + off_qn), fp8 ? (float *)(c + off_qs) : nullptr,
+        s.tau.as<unsigned long long>(), d_dcnt, certify ? d_fullmin : nullptr, d_err);
     PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
 
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
-    if (!g->tmap_x_ok) {
-        if (!tc_make_tmap(&tmX, g->d_vlow, fp8, (uint64_t)g->kpad, g->count)) {
+    bool &x_ok = tf32 ? g->tmap_x32_ok : g->tmap_x_ok;
+    unsigned char *x_map = tf32 ? g->tmap_x32 : g->tmap_x;
+    if (tf32 && g->tmap_x32_rows != g->count) x_ok = false;  // encoded for the current rows
+    if (!x_ok) {
+        const bool okm = tf32 ? tc_make_tmap(&tmX, g->d_vecs, kind, (uint64_t)g->dpad, g->count)
+                              : tc_make_tmap(&tmX, g->d_vlow, kind, (uint64_t)g->kpad, g->count);
+        if (!okm) {
             snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
             return -1;
         }
-        memcpy(g->tmap_x, &tmX, sizeof(tmX));
-        g->tmap_x_ok = true;
+        memcpy(x_map, &tmX, sizeof(tmX));
+        x_ok = true;
+        if (tf32) g->tmap_x32_rows = g->count;
     }
-    memcpy(&tmX, g->tmap_x, sizeof(tmX));
-    if (g->tmap_q_ptr != c || g->tmap_q_rows != (uint64_t)nqpad) {
-        if (!tc_make_tmap(&tmQ, c, fp8, (uint64_t)g->kpad, (uint64_t)nqpad)) {
+    memcpy(&tmX, x_map, sizeof(tmX));
+    if (g->tmap_q_ptr != c || g->tmap_q_rows != (uint64_t)nqpad || g->tmap_q_kind != kind) {
+        if (!tc_make_tmap(&tmQ, c, kind, (uint64_t)kelems, (uint64_t)nqpad)) {
             g->tmap_q_ptr = nullptr;
             snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
             return -1;
@@ -362,6 +399,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         memcpy(g->tmap_q, &tmQ, sizeof(tmQ));
         g->tmap_q_ptr = c;
         g->tmap_q_rows = (uint64_t)nqpad;
+        g->tmap_q_kind = kind;
     }
     memcpy(&tmQ, g->tmap_q, sizeof(tmQ));
     TcArgs a;
@@ -376,7 +414,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.bq = bq;
     a.push_tau = KP == S ? 1 : 0;
     a.NS = NS;
-    a.xnorm = g->d_norm;
+    a.xnorm = tf32 ? g->d_norm32 : g->d_norm;
     a.xscale = fp8 ? g->d_vscale : nullptr;
     a.qnorm = (const float *)(c + off_qn);
     a.qscale = fp8 ? (const float *)(c + off_qs) : nullptr;
@@ -412,8 +450,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         }
     }
     auto run = [&](const TcArgs &args) {
-        return EPI == 2 ? tc_launch<2>(fp8, args.grow * qtiles, smem, g->stream, tmX, tmQ, args)
-                        : tc_launch<1>(fp8, args.grow * qtiles, smem, g->stream, tmX, tmQ, args);
+        return EPI == 2 ? tc_launch<2>(kind, args.grow * qtiles, smem, g->stream, tmX, tmQ, args)
+                        : tc_launch<1>(kind, args.grow * qtiles, smem, g->stream, tmX, tmQ, args);
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
@@ -460,7 +498,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.tile_step = 1;
     PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
-    uint8_t *d_unc = certify ? (uint8_t *)(c + off_unc) : nullptr;
+    uint8_t *d_unc = (certify || num_cert) ? (uint8_t *)(c + off_unc) : nullptr;
     if (S == (int)topb) {
         // certified exact (integer rows and queries, all sums below 2^24):
         // every norm-form distance already is the exact squared L2 distance,
@@ -475,9 +513,16 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                                       d_qprog, popcnt, g->count, nq, cand, ccnt,
                                       (uint8_t *)(c + off_ctr), nullptr, d_unc, g->stream),
                    errbuf, errlen);
+        RerankCert cert;
+        if (num_cert) {
+            cert.qnorm = (const float *)(c + off_qn);
+            cert.xnmax = g->norm32_max;
+            cert.dim = g->dpad;
+            cert.unc = d_unc;
+        }
         rerank_kernel<<<nq, 256, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, S, topb,
                                                  d_qprog, popcnt, g->count, d_out, d_cnt,
-                                                 d_trunc);
+                                                 d_trunc, cert);
         PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
     }
     g->tc_unc = d_unc;

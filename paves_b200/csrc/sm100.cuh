@@ -124,6 +124,17 @@ __device__ __forceinline__ void mma_f8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// same, kind::tf32 (32-bit operands read as tf32: 10 explicit mantissa
+// bits, the low 13 bits of each f32 ignored; f32 acc; 8 elements of K per
+// instruction, i.e. the same 32 bytes of K as the other kinds)
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
 // Arrives on `bar` once all previously issued MMAs of this thread completed.
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile(
@@ -165,6 +176,7 @@ __host__ __device__ constexpr uint32_t idesc_make(uint32_t afmt, uint32_t bfmt, 
 }
 constexpr uint32_t FMT_BF16 = 1;  // kind::f16 operand format
 constexpr uint32_t FMT_E4M3 = 0;  // kind::f8f6f4 operand format
+constexpr uint32_t FMT_TF32 = 2;  // kind::tf32 operand format (A and B alike)
 
 }  // namespace sm100
 }  // namespace pv

@@ -46,10 +46,20 @@ constexpr int TC_MAX_STAGES = 8;   // TMA pipeline stages at most
 constexpr int TC_NR = 8;            // tiles of row norms in flight (shared-memory ring)
 constexpr int TC_NSLOT_F = 2 * TC_BN;  // floats per norm slot: norms, then fp8 scales
 
-template <bool FP8>
-__device__ __forceinline__ void mma_f16_or_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
-                                              uint32_t acc) {
-    if (FP8) mma_f8(d, a, b, idesc, acc);
+// Operand kinds of a pass: rows and queries as BF16, FP8-E4M3 (per-row and
+// per-query scales) or the f32 rows themselves read as TF32.
+constexpr int TCK_BF16 = 0;
+constexpr int TCK_FP8 = 1;
+constexpr int TCK_TF32 = 2;
+__host__ __device__ constexpr int tck_esz(int kind) {
+    return kind == TCK_FP8 ? 1 : kind == TCK_TF32 ? 4 : 2;
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma_kind(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t acc) {
+    if (KIND == TCK_FP8) mma_f8(d, a, b, idesc, acc);
+    else if (KIND == TCK_TF32) mma_tf32(d, a, b, idesc, acc);
     else mma_f16(d, a, b, idesc, acc);
 }
 
@@ -179,7 +189,7 @@ struct TcRun {
 // tiles and passes, so a kernel can run several passes over the same
 // barriers and tensor memory (every role advances the counts alike).
 // Returns false when a wait of this CTA gave up (*abort_flag set).
-template <bool FP8, int EPI>
+template <int KIND, int EPI>
 __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorMap *tmQp,
                                         const TcArgs &a, const TcSmem &sm, uint32_t tmem,
                                         TcRun &run, volatile int *abort_flag, int qtile,
@@ -197,6 +207,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
     float *snorm = sm.snorm;
     uint64_t *full = sm.full, *empty = sm.empty, *tfull = sm.tfull, *tempty = sm.tempty;
     uint64_t *qbar = sm.qbar, *done = sm.done, *nfull = sm.nfull, *nempty = sm.nempty;
+    constexpr bool FP8 = KIND == TCK_FP8;
+    constexpr int BOXE = TC_KB_BYTES / tck_esz(KIND);  // elements of K per box
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // this CTA's tiles: tile0 + t * tile_step, t < ntiles
     const uint64_t tile0 = (uint64_t)rgrp * a.tile0_mul;
@@ -216,7 +228,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             prefetch_tmap(&tmQ);
             mbar_arrive_expect_tx(qbar, (uint32_t)KBt * TC_BOX);
             for (int kb = 0; kb < KBt; kb++)
-                tma_load_2d(sQ + (size_t)kb * TC_BOX, &tmQ, kb * (FP8 ? 128 : 64),
+                tma_load_2d(sQ + (size_t)kb * TC_BOX, &tmQ, kb * BOXE,
                             qtile * TC_BM, qbar);
             const uint32_t nbytes = (FP8 ? 2 : 1) * TC_BN * 4;
             uint64_t it = it0, nt = T0;  // stages and norm slots issued (running)
@@ -248,7 +260,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                     mbar_arrive_expect_tx(&full[s], (uint32_t)nkb * TC_BOX);
                     for (int kb = 0; kb < nkb; kb++)
                         tma_load_2d(sX + (size_t)s * SB + (size_t)kb * TC_BOX, &tmX,
-                                    (kc * TC_KBS + kb) * (FP8 ? 128 : 64), y, &full[s]);
+                                    (kc * TC_KBS + kb) * BOXE, y, &full[s]);
                 }
                 if (a.trace && blockIdx.x == 0 && t < (uint64_t)a.trace_tiles)
                     a.trace[t * 4 + 0] = globaltimer();
@@ -272,7 +284,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = FP8 ? idesc_make(FMT_E4M3, FMT_E4M3, TC_BM, TC_BN)
-                                       : idesc_make(FMT_BF16, FMT_BF16, TC_BM, TC_BN);
+                                   : KIND == TCK_TF32 ? idesc_make(FMT_TF32, FMT_TF32, TC_BM, TC_BN)
+                                                      : idesc_make(FMT_BF16, FMT_BF16, TC_BM, TC_BN);
             bool ok = mbar_wait(qbar, qph, deadline, abort_flag);
             uint64_t it = it0;
             for (uint64_t t = 0; t < ntiles && ok; t++) {
@@ -293,8 +306,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                         const uint64_t bd = desc_sw128(sX + (size_t)s * SB + (size_t)kb * TC_BOX);
 #pragma unroll
                         for (int kk = 0; kk < 4; kk++)  // 4 x 32 bytes of K per block
-                            mma_f16_or_f8<FP8>(dcol, ad + 2 * kk, bd + 2 * kk, idesc,
-                                               (kc | kb | kk) != 0);
+                            mma_kind<KIND>(dcol, ad + 2 * kk, bd + 2 * kk, idesc,
+                                           (kc | kb | kk) != 0);
                     }
                     mma_commit(&empty[s]);
                 }
@@ -389,6 +402,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
 #define PV_L(j) L[(size_t)(j) * NSLOT]
         int n = 0;
         uint64_t lmax = KEY_MAX;   // worst kept key once the list is full
+        uint64_t pushed = KEY_MAX; // last key this list pushed to the grid-wide bound
         uint64_t thr = qvalid ? KEY_MAX : 0ull;  // admission threshold
         float thr_d = qvalid ? __int_as_float(0x7f800000) : -1.f;  // its distance
         bool ok = true;
@@ -520,7 +534,12 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             __syncwarp();
             if (lane == 0) mbar_arrive(&nempty[ns]);
             if (tr) a.trace[t * 4 + 3] = globaltimer();
-            if (a.push_tau && qvalid && n == KP && lmax < KEY_MAX) atomicMin(a.tau + qg, lmax);
+            // a full list's last key bounds the grid-wide bound; pushed only
+            // when it improved (all lists of a query push to one word)
+            if (a.push_tau && qvalid && n == KP && lmax < pushed) {
+                atomicMin(a.tau + qg, lmax);
+                pushed = lmax;
+            }
             return true;
         };
         uint32_t wA[CPH], wB[CPH];
@@ -585,7 +604,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
 // one warp: query row qi of the tile (qi < nqpad)
 __device__ __forceinline__ void query_prep_row(int qi, int lane, const float *__restrict__ q,
                                                int nq, int dpad, int dim, int bq, int kelems,
-                                               bool fp8, unsigned char *__restrict__ out,
+                                               int kind, unsigned char *__restrict__ out,
                                                float *__restrict__ qnorm,
                                                float *__restrict__ qscale,
                                                unsigned long long *__restrict__ tau,
@@ -600,6 +619,7 @@ __device__ __forceinline__ void query_prep_row(int qi, int lane, const float *__
     }
     const int src = qi % bq;
     const bool ok = src < nq;
+    const bool fp8 = kind == TCK_FP8;
     float amax = 0.f;
     if (fp8 && ok)
         for (int j = lane; j < dim; j += 32) amax = fmaxf(amax, fabsf(q[(size_t)src * dpad + j]));
@@ -613,6 +633,11 @@ __device__ __forceinline__ void query_prep_row(int qi, int lane, const float *__
             __nv_fp8_e4m3 b(v / s);
             out[(size_t)qi * kelems + j] = *(unsigned char *)&b;
             r = float(b) * s;
+        } else if (kind == TCK_TF32) {
+            // the f32 value itself (the MMA reads its tf32 part); the norm
+            // is the exact row's
+            ((float *)out)[(size_t)qi * kelems + j] = v;
+            r = v;
         } else {
             __nv_bfloat16 b = __float2bfloat16_rn(v);
             ((__nv_bfloat16 *)out)[(size_t)qi * kelems + j] = b;
@@ -627,6 +652,34 @@ __device__ __forceinline__ void query_prep_row(int qi, int lane, const float *__
     }
 }
 
+// The numerical certificate of a re-ranked superset whose scan distances
+// were inexact (f32 rows read as TF32): qnorm = null turns it off.
+//
+// A row outside the superset has scan key >= the superset's last key A
+// (the merge kept the S smallest keys), so its scan distance is >= A, and
+// its exact distance exceeds the answer's last exact distance Dk if
+//     (A - E) * (1 - c2) > Dk,
+// E bounding |scan distance - true distance| and c2 the relative error of
+// the f32 difference-form sum (the exact distance) against the true one:
+//   * the MMA reads each f32 operand with its low 13 mantissa bits
+//     dropped, a relative change below 2^-10 per operand, so each product
+//     moves by at most (2^-9 + 2^-20) |x_i| |q_i|; the f32 accumulation in
+//     the tensor core adds at most about dim * 2^-22 of sum |x_i q_i|; and
+//     sum |x_i| |q_i| <= ||x|| ||q|| (Cauchy-Schwarz), with ||x||^2 at most
+//     xnmax over all rows;
+//   * the f32 norms (dim terms) and the two roundings of ||x||^2 + ||q||^2
+//     - 2 q.x stay within c2 = (dim + 8) * 2^-23 of the values they round.
+// E = 1.25 * 2^-8 ||q|| sqrt(xnmax) (1 + c2) + c2 (xnmax + ||q||^2 + A)
+// covers both terms with a margin (the first has 2^-8 * 1.25 against the
+// 2^-8 + 2^-19 + dim * 2^-21 the analysis needs for dim <= 128). Queries
+// that fail are flagged in unc[] for an exact re-run.
+struct RerankCert {
+    const float *qnorm = nullptr;  // [nq] ||q||^2 (f32)
+    float xnmax = 0.f;             // max ||x||^2 over the rows (f32 norms)
+    int dim = 0;
+    uint8_t *unc = nullptr;        // [nq] set to 1 when not certified
+};
+
 // One query's re-rank by the block's NT threads (8 lanes per candidate,
 // NT / 8 in flight); keys: TC_MAX_SUPERSET slots of shared memory. Ends
 // with the block synchronized.
@@ -639,10 +692,12 @@ __device__ __forceinline__ void rerank_query(int q, uint64_t *keys, const float 
                                              const unsigned long long *__restrict__ popcnt,
                                              uint64_t nrows, FvHit *__restrict__ out,
                                              uint32_t *__restrict__ out_cnt,
-                                             uint8_t *__restrict__ trunc) {
+                                             uint8_t *__restrict__ trunc,
+                                             const RerankCert cert = RerankCert()) {
     const int tid = threadIdx.x;
     const int grp = tid >> 3, sub = tid & 7;
-    int n = (int)cand_cnt[q];
+    const int ncand = (int)cand_cnt[q];
+    int n = ncand;
     if (n > S) n = S;
     const float *qv = queries + (size_t)q * dpad;
     for (int base = 0; base < n; base += NT / 8) {
@@ -695,6 +750,15 @@ __device__ __forceinline__ void rerank_query(int q, uint64_t *keys, const float 
         const int pg = qprog[q];
         const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
         trunc[q] = passing > (unsigned long long)topb ? 1 : 0;
+        // a superset short of S holds every row that can pass: nothing to certify
+        if (cert.qnorm && ncand >= S && nout == (int)topb) {
+            const double A = (double)cand[(size_t)q * S + (S - 1)].dist;
+            const double Dk = (double)key_dist(keys[nout - 1]);
+            const double qn = (double)cert.qnorm[q], xm = (double)cert.xnmax;
+            const double c2 = (double)(cert.dim + 8) * 0x1p-23;
+            const double E = 1.25 * 0x1p-8 * sqrt(qn * xm) * (1.0 + c2) + c2 * (xm + qn + A);
+            if (!((A - E) * (1.0 - c2) > Dk)) cert.unc[q] = 1;
+        }
     }
     __syncthreads();
 }
@@ -972,8 +1036,9 @@ __device__ __forceinline__ void dense_top32_query(
     __syncthreads();
 }
 
-// host: a 2-D tensor map over [rows][inner] low-precision elements with
-// 128-byte swizzled boxes of [128 rows][128 bytes] (false if encoding failed)
-bool tc_make_tmap(CUtensorMap *m, const void *ptr, bool fp8, uint64_t inner, uint64_t rows);
+// host: a 2-D tensor map over [rows][inner] elements of operand kind `kind`
+// with 128-byte swizzled boxes of [128 rows][128 bytes] (false if encoding
+// failed)
+bool tc_make_tmap(CUtensorMap *m, const void *ptr, int kind, uint64_t inner, uint64_t rows);
 
 }  // namespace pv
