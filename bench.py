@@ -867,22 +867,25 @@ def main():
     per_class = max(1, args.steps // nclass)
 
     def plain_leg():
-        bxs, ms_tot, on_tc = [], 0.0, 0
+        # (stage events: stage 1 is the scan kernel of each batch)
+        bxs, ms_tot, on_tc, scan_tc_ms = [], 0.0, 0, []
         for name, p, q, ent, bp in cls:
             bx = prepared_batch(gi, q, bp, TOPK, _lib.PV_MODE_EXACT)
             batch_run(bx, 3)
-            ms, _ = batch_run(bx, per_class)
-            ms_tot += ms
-            on_tc += L.pv_last_exact_tc(gi.handle)
+            _, st = batch_run(bx, per_class, stages=True)
+            ms_tot += sum(st)
+            if L.pv_last_exact_tc(gi.handle):
+                on_tc += 1
+                scan_tc_ms.append(st[1] / per_class)
             bxs.append(bx)
         ans = [fetch(bx, BATCH, TOPK) for bx in bxs]
         for bx in bxs:
             L.pv_batch_free(bx)
-        return BATCH * per_class * nclass / (ms_tot / 1e3), ans, on_tc
+        return BATCH * per_class * nclass / (ms_tot / 1e3), ans, on_tc, scan_tc_ms
 
-    plain_qps, exact, plain_tc = plain_leg()
+    plain_qps, exact, plain_tc, tf32_ms = plain_leg()
     L.pv_exact_tc(gi.handle, 0)
-    simt_qps, exact_simt, _ = plain_leg()
+    simt_qps, exact_simt, _, _ = plain_leg()
     L.pv_exact_tc(gi.handle, 1)
     simt_same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
                     for a, b in zip(exact, exact_simt))
@@ -1040,6 +1043,16 @@ def main():
                           "tensor_core_batches": f"{plain_tc} of {nclass}",
                           "cuda_cores_only": round(simt_qps, 1),
                           "same_answers_as_cuda_cores": simt_same},
+            # the exact path's dominant kernel: f32 rows (512 B) + f32 norm per row
+            "roofline_exact": None if not tf32_ms else {
+                "bound": "hbm", "kernel": "scan_tc_kernel (TF32)", "unit": "GB/s",
+                "achieved": round(N_ROWS * (DIM * 4 + 4) / (statistics.mean(tf32_ms) / 1e3) / 1e9, 1),
+                "peak": hbm, "peak_kind": peak_kind,
+                "frac": round(N_ROWS * (DIM * 4 + 4) / (statistics.mean(tf32_ms) / 1e3) / 1e9 / hbm, 4),
+                "kernel_ms": round(statistics.mean(tf32_ms), 4),
+                "alg_bytes_per_launch": N_ROWS * (DIM * 4 + 4),
+                "traffic": load_traffic("scan_tc_kernel_tf32"),
+                "traffic_source": "ncu capture of the same kernel (profiles/traffic.json)"},
             "scan_only": {"value": round(scan_only_qps, 1), "unit": "queries/s",
                           "path": "bf16 scan + re-rank (sparse route for selective "
                                   "filters), no router", "classes": per_cls},

@@ -12,6 +12,7 @@
 // small-integer sets, compiled on the host) and cost a few instructions per
 // row; others run on the bit-stack interpreter.
 #include "bitmap_core.cuh"
+#include "launch.cuh"
 
 namespace pv {
 
@@ -23,6 +24,8 @@ bitmap_multi_kernel(const double *__restrict__ cols, uint64_t nrows,
                     const int *__restrict__ dcounts, int ncols,
                     uint32_t *__restrict__ bitmaps, uint64_t bm_words,
                     unsigned long long *__restrict__ popcnt) {
+    pdl_wait();
+    pdl_trigger();
     bitmap_work(blockIdx.x, gridDim.x, cols, nrows, insns, ninsns, progs, P, consts, nconsts,
                 dcounts, ncols, bitmaps, bm_words, popcnt);
 }
@@ -38,10 +41,9 @@ static cudaError_t launch_multi(const double *cols, uint64_t nrows, const PredIn
     const uint64_t cap = (uint64_t)sm_count * BM_BLOCKS_PER_SM;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    bitmap_multi_kernel<<<(unsigned)blocks, 256, 0, st>>>(cols, nrows, insns, ninsns, progs, P,
-                                                          consts, nconsts, dcounts, ncols,
-                                                          bitmaps, bm_words, popcnt);
-    return cudaGetLastError();
+    return launch_pdl(bitmap_multi_kernel, dim3((unsigned)blocks), dim3(256), 0, st, cols, nrows,
+                      insns, ninsns, progs, P, consts, nconsts, dcounts, ncols, bitmaps, bm_words,
+                      popcnt);
 }
 
 cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *insns,

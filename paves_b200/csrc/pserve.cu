@@ -157,7 +157,7 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
         tc_init_barriers(sm, p.NS, EPI);
     }
     if (warp == 1) {
-        tmem_alloc(&s_tmem, 256);
+        tmem_alloc(&s_tmem, TC_TMEM_COLS);
         tmem_relinquish();
     }
     __syncthreads();
@@ -347,7 +347,7 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(s_tmem, 256);
+        tmem_dealloc(s_tmem, TC_TMEM_COLS);
     }
 }
 

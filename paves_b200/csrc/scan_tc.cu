@@ -7,8 +7,8 @@
 // products from one GEMM per 128-row tile:
 //     D[128 queries][128 rows] = Q[128 x K] * X_tile[128 x K]^T
 // (A = query tile, resident in shared memory; B = row tile, streamed by
-// TMA in 128-byte-swizzled K-major boxes). D lives in TMEM, double
-// buffered, so the MMA of tile t+1 overlaps the epilogue of tile t.
+// TMA in 128-byte-swizzled K-major boxes). D lives in TMEM in four
+// buffers, so the MMAs of the next tiles overlap the epilogue of tile t.
 // In TMEM, lane = query and column = row: each epilogue thread owns ONE
 // query, walks the tile's 128 rows and keeps that query's best K' keys
 // in a private shared-memory list with its threshold in a register; the
@@ -39,6 +39,7 @@
 
 #include "pv_internal.h"
 #include "sm100.cuh"
+#include "launch.cuh"
 #include "tc_core.cuh"
 
 namespace pv {
@@ -61,17 +62,19 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         tc_init_barriers(sm, a.NS, EPI);
     }
     if (warp == 1) {
-        tmem_alloc(&s_tmem, 256);
+        tmem_alloc(&s_tmem, TC_TMEM_COLS);
         tmem_relinquish();
     }
     __syncthreads();
     tc_fence_after();
+    pdl_wait();  // the previous kernel's outputs (query tile, bounds, bitmaps)
+    pdl_trigger();
     TcRun run;
     tc_pass<KIND, EPI>(&tmX, &tmQ, a, sm, s_tmem, run, &s_abort, blockIdx.x % a.qtiles,
                       blockIdx.x / a.qtiles);
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(s_tmem, 256);
+        tmem_dealloc(s_tmem, TC_TMEM_COLS);
     }
 }
 
@@ -91,6 +94,8 @@ __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad,
                                   float *__restrict__ qscale, unsigned long long *__restrict__ tau,
                                   uint32_t *__restrict__ dcnt,
                                   unsigned long long *__restrict__ fullmin, int *__restrict__ err) {
+    pdl_wait();
+    pdl_trigger();
     const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (qi >= nqpad) return;
     query_prep_row(qi, threadIdx.x & 31, q, nq, dpad, dim, bq, kelems, kind, out, qnorm, qscale,
@@ -110,6 +115,8 @@ rerank_kernel(const float *__restrict__ vecs, int dpad, const float *__restrict_
               FvHit *__restrict__ out, uint32_t *__restrict__ out_cnt,
               uint8_t *__restrict__ trunc, const RerankCert cert) {
     __shared__ uint64_t keys[TC_MAX_SUPERSET];
+    pdl_wait();
+    pdl_trigger();
     rerank_query<256>(blockIdx.x, keys, vecs, dpad, queries, cand, cand_cnt, S, topb, qprog, popcnt,
                       nrows, out, out_cnt, trunc, cert);
 }
@@ -134,6 +141,8 @@ dense_merge_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, int stage_
                    uint8_t *__restrict__ trunc, unsigned long long *tau_out,
                    uint8_t *__restrict__ unc) {
     extern __shared__ __align__(16) unsigned char dm_smem[];
+    pdl_wait();
+    pdl_trigger();
     dense_merge_query(blockIdx.x, (uint64_t *)dm_smem, dense, dcap, stage_cap, dcnt, reset_cnt,
                       fullmin, tau, KO, qprog, popcnt, nrows, out, out_cnt, trunc, tau_out, unc);
 }
@@ -147,6 +156,8 @@ dense_top32_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
                    uint8_t *__restrict__ trunc, unsigned long long *tau_out,
                    uint8_t *__restrict__ unc) {
     __shared__ uint64_t lists[DM_THREADS / 32][32];
+    pdl_wait();
+    pdl_trigger();
     dense_top32_query(blockIdx.x, lists, dense, dcap, dcnt, reset_cnt, fullmin, tau, KO, qprog,
                       popcnt, nrows, out, out_cnt, trunc, tau_out, unc);
 }
@@ -159,21 +170,18 @@ cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *d
                                unsigned long long *tau_out, uint8_t *unc, cudaStream_t st) {
     if (KO < 1 || KO > DM_OUT) return cudaErrorInvalidValue;
     if (KO <= 32) {
-        dense_top32_kernel<<<nq, DM_THREADS, 0, st>>>(dense, dcap, dcnt, reset_cnt ? 1 : 0,
-                                                      fullmin, tau, KO, qprog, popcnt, nrows, out,
-                                                      out_cnt, trunc, tau_out, unc);
-        return cudaGetLastError();
+        return launch_pdl(dense_top32_kernel, dim3(nq), dim3(DM_THREADS), 0, st, dense, dcap,
+                          dcnt, reset_cnt ? 1 : 0, fullmin, tau, KO, qprog, popcnt, nrows, out,
+                          out_cnt, trunc, tau_out, unc);
     }
     // the stage holds a whole run when it can (runs never exceed dcap)
     const int stage_cap = (int)std::min<uint64_t>(std::max<uint64_t>(dcap, 1), DM_CAP_MAX);
     const size_t smem = (size_t)(stage_cap + DM_OUT) * 8;
     cudaError_t e = raise_smem_limit((const void *)dense_merge_kernel, smem);
     if (e != cudaSuccess) return e;
-    dense_merge_kernel<<<nq, DM_THREADS, smem, st>>>(dense, dcap, stage_cap, dcnt,
-                                                     reset_cnt ? 1 : 0, fullmin, tau, KO, qprog,
-                                                     popcnt, nrows, out, out_cnt, trunc, tau_out,
-                                                     unc);
-    return cudaGetLastError();
+    return launch_pdl(dense_merge_kernel, dim3(nq), dim3(DM_THREADS), smem, st, dense, dcap,
+                      stage_cap, dcnt, reset_cnt ? 1 : 0, fullmin, tau, KO, qprog, popcnt, nrows,
+                      out, out_cnt, trunc, tau_out, unc);
 }
 
 // ---------------------------------------------------------------- host side
@@ -264,8 +272,8 @@ static cudaError_t tc_launch_kind(int grid, size_t smem, cudaStream_t st, const 
                                   const CUtensorMap &tmQ, const TcArgs &a) {
     cudaError_t e = raise_smem_limit((const void *)scan_tc_kernel<KIND, EPI>, smem);
     if (e != cudaSuccess) return e;
-    scan_tc_kernel<KIND, EPI><<<grid, 64 + 128 * EPI, smem, st>>>(tmX, tmQ, a);
-    return cudaGetLastError();
+    return launch_pdl(scan_tc_kernel<KIND, EPI>, dim3(grid), dim3(64 + 128 * EPI), smem, st, tmX,
+                      tmQ, a);
 }
 
 template <int EPI>
@@ -302,17 +310,20 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         return -1;
     }
     // two epilogue warp groups (each row half of a tile) when the lists fit,
-    // with at least two pipeline stages; else one group
+    // with at least two pipeline stages; else one group. The automatic shape
+    // stays within smem_pref, which leaves each SM a few KB for a small
+    // kernel beside the scan (the router's, a merge launched early).
     const size_t smem_cap = 227 * 1024;
+    const size_t smem_pref = 222 * 1024;
     // stages: up to 128 KB of rows in flight
     const int ns0 = std::min(TC_MAX_STAGES, std::max(
         2, (int)(128 * 1024 / ((size_t)std::min(kblocks, TC_KBS) * TC_BOX))));
     int EPI = 2, NS = ns0;
-    while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
-    if (tc_smem(kblocks, NS, KP, EPI) > smem_cap) {
+    while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_pref) NS--;
+    if (tc_smem(kblocks, NS, KP, EPI) > smem_pref) {
         EPI = 1;
         NS = ns0;
-        while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_cap) NS--;
+        while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_pref) NS--;
     }
     if (g->tune_epi || g->tune_ns) {  // a tuned shape, if it fits
         const int e = g->tune_epi ? g->tune_epi : EPI, n = g->tune_ns ? g->tune_ns : NS;
@@ -367,11 +378,12 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const bool num_cert = tf32 && S > (int)topb;
 
     g->launches += 4;  // query prep, main pass, merge, re-rank
-    query_prep_kernel<<<(nqpad + 7) / 8, 256, 0, g->stream>>>(
-        d_q, nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, kelems, kind, c,
-        (float *)(c + off_qn), fp8 ? (float *)(c + off_qs) : nullptr,
-        s.tau.as<unsigned long long>(), d_dcnt, certify ? d_fullmin : nullptr, d_err);
-    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    PV_CUDA_OK(launch_pdl(query_prep_kernel, dim3((nqpad + 7) / 8), dim3(256), 0, g->stream, d_q,
+                          nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, kelems, kind, c,
+                          (float *)(c + off_qn), fp8 ? (float *)(c + off_qs) : nullptr,
+                          s.tau.as<unsigned long long>(), d_dcnt,
+                          certify ? d_fullmin : nullptr, d_err),
+               errbuf, errlen);
 
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
@@ -520,10 +532,10 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
             cert.dim = g->dpad;
             cert.unc = d_unc;
         }
-        rerank_kernel<<<nq, 256, 0, g->stream>>>(g->d_vecs, g->dpad, d_q, cand, ccnt, S, topb,
-                                                 d_qprog, popcnt, g->count, d_out, d_cnt,
-                                                 d_trunc, cert);
-        PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+        PV_CUDA_OK(launch_pdl(rerank_kernel, dim3(nq), dim3(256), 0, g->stream, g->d_vecs,
+                              g->dpad, d_q, cand, ccnt, S, topb, d_qprog, popcnt, g->count, d_out,
+                              d_cnt, d_trunc, cert),
+                   errbuf, errlen);
     }
     g->tc_unc = d_unc;
     g->tc_unc_n = nq;

@@ -4,8 +4,8 @@
 // A pass streams one query tile against a CTA's row tiles:
 //     D[128 queries][128 rows] = Q[128 x K] * X_tile[128 x K]^T
 // (A = query tile, resident in shared memory; B = row tile, streamed by
-// TMA in 128-byte-swizzled K-major boxes), D in TMEM, double buffered, so
-// the MMA of tile t+1 overlaps the epilogue of tile t. In TMEM, lane =
+// TMA in 128-byte-swizzled K-major boxes), D in TMEM, four buffers, so
+// the MMAs of tiles t+1..t+3 overlap the epilogue of tile t. In TMEM, lane =
 // query and column = row: each epilogue thread owns ONE query, walks the
 // tile's rows and keeps that query's best K' keys in a private
 // shared-memory list with its threshold in a register. Row norms (and FP8
@@ -45,6 +45,12 @@ constexpr int TC_MAX_LIST = 64;
 constexpr int TC_MAX_STAGES = 8;   // TMA pipeline stages at most
 constexpr int TC_NR = 8;            // tiles of row norms in flight (shared-memory ring)
 constexpr int TC_NSLOT_F = 2 * TC_BN;  // floats per norm slot: norms, then fp8 scales
+// TMEM accumulators (128 columns each, all 512 of the SM's): the MMA of a
+// tile waits only for the epilogue of the tile NACC back, so the MMA's own
+// latency (issue to completion ~1 us for a BF16 tile) overlaps up to three
+// epilogues instead of one
+constexpr int TC_NACC = 4;
+constexpr uint32_t TC_TMEM_COLS = TC_NACC * TC_BN;
 
 // Operand kinds of a pass: rows and queries as BF16, FP8-E4M3 (per-row and
 // per-query scales) or the f32 rows themselves read as TF32.
@@ -141,9 +147,9 @@ __device__ __forceinline__ TcSmem tc_carve(unsigned char *base, int KBt, int NS,
     uint64_t *bars = (uint64_t *)(m.snorm + (size_t)TC_NR * TC_NSLOT_F);
     m.full = bars;              // [NS]
     m.empty = m.full + NS;      // [NS]
-    m.tfull = m.empty + NS;     // [2]
-    m.tempty = m.tfull + 2;     // [2]
-    m.qbar = m.tempty + 2;      // [1]
+    m.tfull = m.empty + NS;           // [TC_NACC]
+    m.tempty = m.tfull + TC_NACC;     // [TC_NACC]
+    m.qbar = m.tempty + TC_NACC;      // [1]
     m.done = m.qbar + 1;        // [1]
     m.nfull = m.done + 1;       // [TC_NR]
     m.nempty = m.nfull + TC_NR; // [TC_NR]
@@ -154,7 +160,7 @@ inline size_t tc_smem_bytes(int kblocks, int NS, int KPcap, int EPI) {
     return 1024 + (size_t)kblocks * TC_BOX +
            (size_t)NS * (kblocks < TC_KBS ? kblocks : TC_KBS) * TC_BOX +
            (size_t)TC_BM * EPI * KPcap * 8 + (size_t)32 * TC_BM * EPI * 4 +
-           (size_t)TC_NR * TC_NSLOT_F * 4 + (size_t)(2 * NS + 6 + 2 * TC_NR) * 8;
+           (size_t)TC_NR * TC_NSLOT_F * 4 + (size_t)(2 * NS + 2 * TC_NACC + 2 + 2 * TC_NR) * 8;
 }
 
 // by one thread, before the CTA's first pass
@@ -163,7 +169,7 @@ __device__ __forceinline__ void tc_init_barriers(const TcSmem &m, int NS, int EP
         mbar_init(&m.full[i], 1);
         mbar_init(&m.empty[i], 1);
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < TC_NACC; i++) {
         mbar_init(&m.tfull[i], 1);
         mbar_init(&m.tempty[i], TC_BM * EPI);
     }
@@ -290,8 +296,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             uint64_t it = it0;
             for (uint64_t t = 0; t < ntiles && ok; t++) {
                 const uint64_t T = T0 + t;
-                const int acc = (int)(T & 1);
-                const uint32_t aph = (uint32_t)((T >> 1) & 1);
+                const int acc = (int)(T % TC_NACC);
+                const uint32_t aph = (uint32_t)((T / TC_NACC) & 1);
                 if (!mbar_wait(&tempty[acc], aph ^ 1, deadline, abort_flag)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t dcol = tmem + (uint32_t)acc * TC_BN;
@@ -430,8 +436,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                              uint32_t (&nbw)[CPH], unsigned long long &ngt) -> bool {
             if (t + 1 < ntiles) load_words(t + 1, nbw, ngt);
             const uint64_t T = T0 + t;  // running tile count: barrier phases
-            const int acc = (int)(T & 1);
-            const uint32_t aph = (uint32_t)((T >> 1) & 1);
+            const int acc = (int)(T % TC_NACC);
+            const uint32_t aph = (uint32_t)((T / TC_NACC) & 1);
             const int ns = (int)(T % TC_NR);
             if (!mbar_wait(&tfull[acc], aph, deadline, abort_flag)) return false;
             if (!mbar_wait(&nfull[ns], (uint32_t)((T / TC_NR) & 1), deadline, abort_flag))
