@@ -304,6 +304,9 @@ KERNEL_CASES = {
     # the same on the CUDA cores alone (pv_exact_tc off)
     "exact_b64_cuda": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, None),
     "bf16_b64": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, None),
+    # one selective class per batch: the sparse route (0.1 %, 1 %)
+    "bf16_b64_sel01": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 0),
+    "bf16_b64_sel1": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 1),
     "fp8_b64": (64, _lib.FV_GPU_PREC_FP8, _lib.PV_MODE_LOW, None),
     # graph: 200k x 128 rows, HNSW M=16 efC=100, 64 queries, 10% filter, ef 64
     "graph_b64": (64, None, None, None),
@@ -914,7 +917,7 @@ def main():
     for i in range(args.steps):
         c = i % nclass
         ids, dists, cnt, dec, ex, st = routed(c)
-        dev_ms += float(st[0] + st[2])  # routing runs beside the search
+        dev_ms += float(st[0] + st[2])  # bitmaps, then the search (routing beside)
         cls_ms.setdefault(c, []).append(float(st[0] + st[2]))
         st_sum += st
         launches += int(L.pv_last_launches(gi.handle))
@@ -1034,7 +1037,7 @@ def main():
             "graph_batches": graph_steps,
             "mixed_batches": mixed_steps,
             "routed_stage_ms": {"bitmaps": round(st_sum[0] / args.steps, 4),
-                                "routing_beside_search": round(st_sum[1] / args.steps, 4),
+                                "routing_after_bitmaps": round(st_sum[1] / args.steps, 4),
                                 "search": round(st_sum[2] / args.steps, 4)},
             "plain_gpu": {"value": round(plain_qps, 1), "unit": "queries/s",
                           "path": "exact FP32 results: f32 rows read as TF32 on the tensor "

@@ -123,9 +123,21 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     g->last_sparse = 0;
     g->last_exact_tc = 0;
     if (db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024) {
+        g->last_sparse = 1;
+        // the matching rows on the tensor cores, when the mode scans there
+        const bool low_tc = mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0;
+        const bool exact_tc = mode == PV_MODE_EXACT && nq >= PV_EXACT_TC_MIN_NQ &&
+                              tf32_supported(g) && tf32_superset(g, topb, db.q_amax) > 0;
+        if ((low_tc || exact_tc) && db.sparse_bound >= PV_SPARSE_TC_MIN_ROWS) {
+            if (sparse_tc_launch(g, db, topb, db.sparse_bound, exact_tc, d_out, d_cnt, d_trunc,
+                                 ev, errbuf, errlen))
+                return -1;
+            g->last_exact_tc = exact_tc ? 1 : 0;
+            if (ev) cudaEventRecord(ev[4], g->stream);
+            return 0;
+        }
         g->tc_err = nullptr;
         g->tc_unc = nullptr;
-        g->last_sparse = 1;
         if (ev) cudaEventRecord(ev[1], g->stream);
         if (sparse_launch(g, db, topb, db.sparse_bound, d_out, d_cnt, d_trunc, errbuf, errlen))
             return -1;

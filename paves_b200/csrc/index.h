@@ -129,6 +129,11 @@ struct FvGpuIndex {
     alignas(64) unsigned char tmap_x[128] = {};
     alignas(64) unsigned char tmap_q[128] = {};
     alignas(64) unsigned char tmap_x32[128] = {};  // the f32 rows (exact mode)
+    alignas(64) unsigned char tmap_c[128] = {};    // a compacted row set (sparse route)
+    bool tmap_c_ok = false;
+    const void *tmap_c_ptr = nullptr;
+    uint64_t tmap_c_rows = 0;
+    int tmap_c_kind = -1;
     bool tmap_x_ok = false;
     bool tmap_x32_ok = false;
     uint64_t tmap_x32_rows = 0;

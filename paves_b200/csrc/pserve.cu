@@ -247,6 +247,8 @@ pserve_kernel(const __grid_constant__ CUtensorMap tmX, SvArgs p) {
         a.nconsts = pl.nconsts;
         a.cols = p.cols;
         a.ncols = p.ncols;
+        a.rowids = nullptr;
+        a.nrows_dev = nullptr;
         a.tau = p.tau;
         a.dense = p.dense;
         a.dcnt = p.dcnt;
@@ -672,7 +674,7 @@ bool sv_plan(PvServe *s, int nq, uint32_t topb, float q_amax, SvPlan &pl) {
     pl.nqpad = pl.qtiles * TC_BM;
     int R = 1;
     if (pl.qtiles == 1) R = nq <= 32 ? 4 : nq <= 64 ? 2 : 1;
-    while (R > 1 && (TC_BM / R < nq || TC_BN / (s->EPI * R) < 32)) R >>= 1;
+    while (R > 1 && (TC_BM / R < nq || TC_BN / R < 32)) R >>= 1;
     pl.rep = R;
     pl.bq = pl.qtiles == 1 && R > 1 ? TC_BM / R : pl.nqpad;
     const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;

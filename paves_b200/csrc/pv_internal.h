@@ -130,6 +130,14 @@ double prog_pass_estimate(const FvGpuIndex *g, const PredInsn *ins, int n, const
 // selective filter leaves a loose threshold (few passing rows), so only
 // programs estimated to pass at least this fraction are tested lazily
 constexpr double PV_LAZY_MIN_PASS = 0.125;
+// Sparse batches whose filter matches at least this many rows (bounded on
+// the host) scan their compacted rows on the tensor cores when the batch's
+// mode can (sparse_tc_launch); smaller ones compute every listed row's
+// exact distance on the CUDA cores (sparse_launch).
+constexpr uint64_t PV_SPARSE_TC_MIN_ROWS = 2048;
+int sparse_tc_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, bool tf32,
+                     FvHit *d_out, uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev,
+                     char *errbuf, size_t errlen);
 int sparse_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, FvHit *d_out,
                   uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen);
 int tc_redo_uncertain(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
@@ -163,12 +171,26 @@ struct TcLazy {
     const double *consts;
     int nconsts;
 };
+// A compacted row set for the tensor-core scan (the sparse route): nrows
+// rows (a multiple of 128) in the scan's operand layout (low-precision rows
+// of kpad elements, or f32 rows of dpad), their norms (and fp8 scales), and
+// the index row of each (keys carry the index row). The batch's bitmaps
+// then mark which compacted rows are valid.
+struct TcRowSet {
+    const void *rows;
+    const float *norms;
+    const float *scales;
+    uint64_t nrows;
+    const uint32_t *rowids;
+    const unsigned long long *nrows_dev;  // rows that exist (device), <= nrows
+};
 int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const int32_t *d_qprog,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen, const TcLazy *lz = nullptr, bool tf32 = false);
+                   size_t errlen, const TcLazy *lz = nullptr, bool tf32 = false,
+                   const TcRowSet *rs = nullptr);
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);

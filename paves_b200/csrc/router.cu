@@ -843,6 +843,195 @@ __global__ void router_decide_kernel(const float *__restrict__ Z3, int nq,
     efq[q] = (uint16_t)ef;
 }
 
+// The routing decision of a batch in two short launches, for the routed
+// batch call (the first beside the bitmaps, the second beside the start of
+// the search). Same features, network and
+// decision rule as router_features_kernel -> mlp_infer_kernel ->
+// router_decide_kernel; the centroid distances are summed in another order
+// (lanes over dimensions, then a shuffle tree), so feature values may
+// differ from those kernels' in the last bits.
+//
+// Step 1: CTA (chunk, query) scores centroid chunk `chunk` (RT_CHUNKS of
+// them) for its query with 4 warps, four centroids per warp at a time, and
+// writes the chunk's 8 smallest squared distances to part[q][chunk][8].
+constexpr int RT_CHUNKS = 8;
+
+__global__ void __launch_bounds__(128) router_cent_kernel(const float *__restrict__ queries,
+                                                          int dpad,
+                                                          const float *__restrict__ cent,
+                                                          int ncent, float *__restrict__ part) {
+    __shared__ float cand[4][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = blockIdx.y, chunk = blockIdx.x;
+    const int per = (ncent + RT_CHUNKS - 1) / RT_CHUNKS;
+    const int cb = chunk * per, ce = min(ncent, cb + per);
+    const float *qv = queries + (uint64_t)q * dpad;
+    float top[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) top[i] = INFINITY;
+    int mine_i = 0;  // the warp's centroids scored so far; lane mine_i % 32 keeps each
+    for (int c0 = cb + warp; c0 < ce; c0 += 16) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int j = lane * 4; j < dpad; j += 128) {
+            const float4 u = *(const float4 *)(qv + j);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int c = c0 + 4 * k;
+                if (c >= ce) break;
+                const float4 v = __ldg((const float4 *)(cent + (uint64_t)c * dpad + j));
+                const float d0 = v.x - u.x, d1 = v.y - u.y, d2 = v.z - u.z, d3 = v.w - u.w;
+                acc[k] = fmaf(d0, d0, acc[k]);
+                acc[k] = fmaf(d1, d1, acc[k]);
+                acc[k] = fmaf(d2, d2, acc[k]);
+                acc[k] = fmaf(d3, d3, acc[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int o = 16; o; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (c0 + 4 * k >= ce) break;
+            if (lane == (mine_i & 31) && acc[k] < top[7]) {
+                float v = acc[k];
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const float t = top[i];
+                    const bool sw = v < t;
+                    top[i] = sw ? v : t;
+                    v = sw ? t : v;
+                }
+            }
+            mine_i++;
+        }
+    }
+    {
+        int head = 0;
+        float mine = INFINITY;
+        for (int r = 0; r < 8; r++) {
+            float best = head < 8 ? pick8(top, head) : INFINITY;
+            int who = lane;
+            warp_argmin(best, who);
+            if (lane == who) head++;
+            if (lane == r) mine = best;
+        }
+        if (lane < 8) cand[warp][lane] = mine;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        float v = cand[lane >> 3][lane & 7];
+        float out = INFINITY;
+        for (int r = 0; r < 8; r++) {
+            float best = v;
+            int who = lane;
+            warp_argmin(best, who);
+            if (lane == who) v = INFINITY;
+            if (lane == r) out = best;
+        }
+        if (lane < 8) part[((uint64_t)q * RT_CHUNKS + chunk) * 8 + lane] = out;
+    }
+}
+
+// Step 2: one warp per query: the 8 smallest over the chunks, the features,
+// the network and the decision.
+__global__ void __launch_bounds__(256) router_route_kernel(
+    const float *__restrict__ queries, int dpad, const float *__restrict__ part,
+    const unsigned long long *__restrict__ popcnt, const int32_t *__restrict__ qprog,
+    uint64_t nrows, const uint32_t *__restrict__ kq, const int32_t *__restrict__ kind,
+    const __nv_bfloat16 *__restrict__ w, const float *__restrict__ norm, float margin, int nq,
+    float *__restrict__ feats, float *__restrict__ Z3, uint16_t *__restrict__ efq) {
+    const int lane = threadIdx.x & 31;
+    const int q = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+    if (q >= nq) return;
+    const float *qv = queries + (uint64_t)q * dpad;
+    float mine = INFINITY;
+    {
+        const float *pq = part + (uint64_t)q * RT_CHUNKS * 8;
+        float v0 = pq[lane], v1 = pq[32 + lane];  // RT_CHUNKS * 8 = 64 candidates
+        for (int r = 0; r < 8; r++) {
+            float best = fminf(v0, v1);
+            int who = lane;
+            warp_argmin(best, who);
+            if (lane == who) {  // remove one occurrence of the minimum
+                if (v0 <= v1) v0 = INFINITY;
+                else v1 = INFINITY;
+            }
+            if (lane == r) mine = best;
+        }
+    }
+    // |q|
+    float s = 0.f;
+    for (int j = lane; j < dpad; j += 32) s = fmaf(qv[j], qv[j], s);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const float qnorm = sqrtf(s);
+    // features: lane i holds feature i
+    float f = 0.f;
+    const float m2 = __shfl_sync(0xffffffffu, mine, (lane + 30) & 31);  // lane - 2
+    if (lane >= 2 && lane < 10) f = sqrtf(m2);
+    if (lane == 0) {
+        const int pg = qprog[q];
+        const double sel = pg < 0 ? 1.0 : (double)popcnt[pg] / (double)nrows;
+        f = (float)log10(sel > 1e-6 ? sel : 1e-6);
+    }
+    if (lane == 1) f = qnorm;
+    if (lane == 10) f = log2f((float)(kq[q] > 0 ? kq[q] : 1));
+    if (lane == 11) f = (float)kind[q];
+    if (feats && lane < NI) feats[(uint64_t)q * NI + lane] = f;
+    // MLP (as mlp_infer_kernel): lanes over the hidden units
+    const float xi = lane < NI ? (f - __ldg(norm + lane)) / __ldg(norm + NI + lane) : 0.f;
+    float h0 = __bfloat162float(w[P_B1 + lane]), h1 = __bfloat162float(w[P_B1 + lane + 32]);
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const float xb = __shfl_sync(0xffffffffu, xi, i);
+        h0 = fmaf(xb, __bfloat162float(w[P_W1 + i * NH + lane]), h0);
+        h1 = fmaf(xb, __bfloat162float(w[P_W1 + i * NH + lane + 32]), h1);
+    }
+    h0 = fmaxf(h0, 0.f);
+    h1 = fmaxf(h1, 0.f);
+    float g0 = __bfloat162float(w[P_B2 + lane]), g1 = __bfloat162float(w[P_B2 + lane + 32]);
+#pragma unroll 8
+    for (int i = 0; i < NH; i++) {
+        const float hb = __shfl_sync(0xffffffffu, i < 32 ? h0 : h1, i & 31);
+        g0 = fmaf(hb, __bfloat162float(w[P_W2 + i * NH + lane]), g0);
+        g1 = fmaf(hb, __bfloat162float(w[P_W2 + i * NH + lane + 32]), g1);
+    }
+    g0 = fmaxf(g0, 0.f);
+    g1 = fmaxf(g1, 0.f);
+    float z[NO];
+#pragma unroll
+    for (int o = 0; o < NO; o++) {
+        float p = g0 * __bfloat162float(w[P_W3 + lane * NO + o]);
+        p = fmaf(g1, __bfloat162float(w[P_W3 + (lane + 32) * NO + o]), p);
+#pragma unroll
+        for (int x = 16; x; x >>= 1) p += __shfl_xor_sync(0xffffffffu, p, x);
+        z[o] = p + __bfloat162float(w[P_B3 + o]);
+    }
+    if (lane == 0) {
+        // the decision rule of router_decide_kernel
+        float mx = -INFINITY;
+#pragma unroll
+        for (int o = 0; o < NO; o++) {
+            if (Z3) Z3[(uint64_t)q * NO + o] = z[o];
+            mx = fmaxf(mx, z[o]);
+        }
+        int a = 0;
+#pragma unroll
+        for (int o = 1; o < NO; o++)
+            if (z[o] > z[a]) a = o;
+        float se = 0.f;
+#pragma unroll
+        for (int o = 0; o < NO; o++) se += expf(z[o] - mx);
+        if (a > 0 && expf(z[a] - mx) - expf(z[0] - mx) < margin * se) a = 0;
+        const int efs[NO] = {0, 32, 64, 128, 256};
+        int ef = efs[a];
+        const int k = (int)kq[q];
+        if (ef > 0 && ef < k) ef = k;
+        if (ef > FV_GPU_MAX_EF) ef = 0;
+        efq[q] = (uint16_t)ef;
+    }
+}
+
 }  // namespace pv
 
 extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *queries,
@@ -919,16 +1108,38 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     const size_t fb = ((size_t)nq * NI * 4 + 255) & ~(size_t)255;
     const size_t zb = ((size_t)nq * NO * 4 + 255) & ~(size_t)255;
     const size_t eb = ((size_t)nq * 2 + 255) & ~(size_t)255;
+    const size_t pb8 = (size_t)nq * RT_CHUNKS * 8 * 4;  // centroid chunk minima
     const size_t gbytes = have_graph ? graph_out_layout(nq, FV_GPU_MAX_EF).bytes : 0;
     RT_OK(s.out_d.ensure(obytes));
     RT_OK(s.out_h.ensure(obytes));
-    RT_OK(g->graph.route.ensure(fb + zb + eb));
+    RT_OK(g->graph.route.ensure(fb + zb + eb + pb8));
     RT_OK(g->graph.route_h.ensure(eb + gbytes));
     if (have_graph) RT_OK(g->graph.gout.ensure(gbytes));
-    RT_OK(cudaEventRecord(ev[0], g->stream));
+    float *dfeat = g->graph.route.as<float>();
+    float *dz = (float *)(g->graph.route.as<char>() + fb);
+    uint16_t *defq = (uint16_t *)(g->graph.route.as<char>() + fb + zb);
+    float *dpart = (float *)(g->graph.route.as<char>() + fb + zb + eb);
+    uint16_t *hefq = g->graph.route_h.as<uint16_t>();
+    if (!plan && g->dpad != r->dpad) {
+        if (errbuf && errlen) snprintf(errbuf, errlen, "routed: router dimension mismatch");
+        return -1;
+    }
     RT_OK(s.popcnt.ensure((size_t)(P > 0 ? P : 1) * 8));
+    if (P > 0) RT_OK(s.bitmaps.ensure((size_t)P * bm_words * 4));
+    RT_OK(cudaEventRecord(ev[0], g->stream));
+    // Routing on the side stream, beside the bitmaps and then the search:
+    // the centroid distances need only the queries (they run while the
+    // bitmaps are built), the features, network and decision need the
+    // bitmaps' counts (a few warps per query); the decisions are read back
+    // into pinned memory while the search runs. (One CTA per query that
+    // held its SM through the scan took issue slots from the scan's
+    // epilogue; on the search stream, in series, it added its latency.)
+    RT_OK(cudaStreamWaitEvent(side, ev[0], 0));
+    g->launches += plan ? 1 : 2;
+    if (!plan)
+        router_cent_kernel<<<dim3(RT_CHUNKS, nq), 128, 0, side>>>(
+            (const float *)(d + db.off_q), g->dpad, r->d_cent, r->ncent, dpart);
     if (P > 0) {
-        RT_OK(s.bitmaps.ensure((size_t)P * bm_words * 4));
         g->launches++;
         RT_OK(launch_bitmaps(g->d_cols, g->count, (const PredInsn *)(d + db.off_insns),
                              (const PredProg *)(d + db.off_progs),
@@ -937,26 +1148,19 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                              db.ninsns, db.nconsts, g->ncols));
     }
     RT_OK(cudaEventRecord(ev[1], g->stream));
-    // Router on the side stream: features -> logits -> beam width per query
-    // (0 = scan), read back into pinned memory.
-    float *dfeat = g->graph.route.as<float>();
-    float *dz = (float *)(g->graph.route.as<char>() + fb);
-    uint16_t *defq = (uint16_t *)(g->graph.route.as<char>() + fb + zb);
-    uint16_t *hefq = g->graph.route_h.as<uint16_t>();
     RT_OK(cudaStreamWaitEvent(side, ev[1], 0));
-    g->launches += plan ? 1 : 3;  // (features, MLP,) decision
     if (!plan) {
-        RT_OK(launch_router_features(r, (const float *)(d + db.off_q), g->dpad, nq,
-                                     s.popcnt.as<unsigned long long>(),
-                                     (const int32_t *)(d + db.off_qprog), g->count,
-                                     (const uint32_t *)dx, (const int32_t *)(dx + n4), dfeat,
-                                     side));
-        RT_OK(launch_router_forward(r, dfeat, nq, dz, side));
+        router_route_kernel<<<(nq + 7) / 8, 256, 0, side>>>(
+            (const float *)(d + db.off_q), g->dpad, dpart,
+            s.popcnt.as<unsigned long long>(), (const int32_t *)(d + db.off_qprog), g->count,
+            (const uint32_t *)dx, (const int32_t *)(dx + n4), r->mlp.w, r->mlp.norm, margin, nq,
+            dfeat, dz, defq);
+    } else {
+        router_decide_kernel<<<(nq + 127) / 128, 128, 0, side>>>(
+            dz, nq, (const uint32_t *)dx, (const uint16_t *)(dx + 3 * n4), margin, defq);
     }
-    router_decide_kernel<<<(nq + 127) / 128, 128, 0, side>>>(
-        dz, nq, (const uint32_t *)dx, plan ? (const uint16_t *)(dx + 3 * n4) : nullptr, margin,
-        defq);
     RT_OK(cudaGetLastError());
+    RT_OK(cudaEventRecord(ev[5], side));
     RT_OK(cudaMemcpyAsync(hefq, defq, (size_t)nq * 2, cudaMemcpyDeviceToHost, side));
     RT_OK(cudaEventRecord(ev[2], side));
     // Speculative scan on the main stream meanwhile: a scan costs about the
@@ -1055,11 +1259,12 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     }
     g->tc_unc = nullptr;
     if (ngraph > 0) done = ev[4];
-    // device time of the batch: bitmaps, then the search with the routing
-    // beside it (t[1] overlaps t[2]; the batch took t[0] + t[2])
+    // device time of the batch: the bitmaps, then the search with the
+    // routing's tail beside it (t[1]: the routing after the bitmaps; the
+    // batch took t[0] + t[2])
     float t[3] = {0, 0, 0}, tot = 0.f;
     cudaEventElapsedTime(&t[0], ev[0], ev[1]);
-    cudaEventElapsedTime(&t[1], ev[1], ev[2]);
+    cudaEventElapsedTime(&t[1], ev[1], ev[5]);
     cudaEventElapsedTime(&tot, ev[0], done);
     if (ngraph > 0 && spec) {
         float a = 0.f;  // the scan may finish last

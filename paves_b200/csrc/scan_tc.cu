@@ -23,7 +23,7 @@
 //
 // Warp roles (64 + 128 * EPI threads): warp 0 TMA producer, warp 1 TMEM
 // allocator + MMA issuer, then EPI groups of 4 epilogue warps (warp w reads
-// TMEM lanes 32*(w%4)..+31; group h takes its share of each tile's rows).
+// TMEM lanes 32*(w%4)..+31; group h owns the tiles h, h + EPI, ...).
 // A batch of at most 64 (32) queries is replicated 2 (4) times down the
 // 128 query slots of the A tile: the MMA costs the same, and each replica
 // takes a disjoint share of every tile's rows, so the epilogue work per
@@ -293,7 +293,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen, const TcLazy *lz, bool tf32) {
+                   size_t errlen, const TcLazy *lz, bool tf32, const TcRowSet *rs) {
     const bool fp8 = !tf32 && g->precision == FV_GPU_PREC_FP8;
     const int kind = tf32 ? TCK_TF32 : fp8 ? TCK_FP8 : TCK_BF16;
     const int esz = tck_esz(kind);
@@ -305,7 +305,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
     g->last_superset = S;
     g->tc_unc = nullptr;
-    if (!S || !(tf32 ? tf32_supported(g) : tc_supported(g))) {
+    if (!S || !(tf32 ? tf32_supported(g) : tc_supported(g)) || (rs && lz)) {
         snprintf(errbuf, errlen, "gpu: tensor-core scan not available for this batch");
         return -1;
     }
@@ -341,9 +341,11 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     int R = 1;
     if (g->tune_rep > 0) R = g->tune_rep;
     else if (qtiles == 1) R = nq <= 32 ? 4 : nq <= 64 ? 2 : 1;
-    while (R > 1 && (TC_BM / R < nq || TC_BN / (EPI * R) < 32)) R >>= 1;
+    while (R > 1 && (TC_BM / R < nq || TC_BN / R < 32)) R >>= 1;
     const int bq = TC_BM / R;
-    const uint64_t ntiles_all = (g->count + TC_BN - 1) / TC_BN;
+    // rows scanned: the index's, or a compacted set
+    const uint64_t nrows_scan = rs ? rs->nrows : g->count;
+    const uint64_t ntiles_all = (nrows_scan + TC_BN - 1) / TC_BN;
     int grow = g->tune_grow > 0 ? g->tune_grow : g->sm_count / qtiles;
     if (grow < 1) grow = 1;
     uint64_t maxg = (ntiles_all + 3) / 4;
@@ -387,9 +389,22 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
 
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
-    bool &x_ok = tf32 ? g->tmap_x32_ok : g->tmap_x_ok;
-    unsigned char *x_map = tf32 ? g->tmap_x32 : g->tmap_x;
-    if (tf32 && g->tmap_x32_rows != g->count) x_ok = false;  // encoded for the current rows
+    bool &x_ok = rs ? g->tmap_c_ok : tf32 ? g->tmap_x32_ok : g->tmap_x_ok;
+    unsigned char *x_map = rs ? g->tmap_c : tf32 ? g->tmap_x32 : g->tmap_x;
+    if (tf32 && !rs && g->tmap_x32_rows != g->count) x_ok = false;  // encoded for the current rows
+    if (rs && (g->tmap_c_ptr != rs->rows || g->tmap_c_rows != rs->nrows || g->tmap_c_kind != kind))
+        x_ok = false;
+    if (rs && !x_ok) {
+        if (!tc_make_tmap(&tmX, rs->rows, kind, (uint64_t)(tf32 ? g->dpad : g->kpad), rs->nrows)) {
+            snprintf(errbuf, errlen, "gpu: tensor map encoding failed");
+            return -1;
+        }
+        memcpy(x_map, &tmX, sizeof(tmX));
+        x_ok = true;
+        g->tmap_c_ptr = rs->rows;
+        g->tmap_c_rows = rs->nrows;
+        g->tmap_c_kind = kind;
+    }
     if (!x_ok) {
         const bool okm = tf32 ? tc_make_tmap(&tmX, g->d_vecs, kind, (uint64_t)g->dpad, g->count)
                               : tc_make_tmap(&tmX, g->d_vlow, kind, (uint64_t)g->kpad, g->count);
@@ -415,7 +430,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     }
     memcpy(&tmQ, g->tmap_q, sizeof(tmQ));
     TcArgs a;
-    a.nrows = g->count;
+    a.nrows = nrows_scan;
     a.kblocks = kblocks;
     a.nq = nq;
     a.qtiles = qtiles;
@@ -426,8 +441,10 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     a.bq = bq;
     a.push_tau = KP == S ? 1 : 0;
     a.NS = NS;
-    a.xnorm = tf32 ? g->d_norm32 : g->d_norm;
-    a.xscale = fp8 ? g->d_vscale : nullptr;
+    a.xnorm = rs ? rs->norms : tf32 ? g->d_norm32 : g->d_norm;
+    a.xscale = fp8 ? (rs ? rs->scales : g->d_vscale) : nullptr;
+    a.rowids = rs ? rs->rowids : nullptr;
+    a.nrows_dev = rs ? rs->nrows_dev : nullptr;
     a.qnorm = (const float *)(c + off_qn);
     a.qscale = fp8 ? (const float *)(c + off_qs) : nullptr;
     a.qprog = d_qprog;
@@ -506,8 +523,11 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     // stage boundary: everything before the main pass (bitmaps, query prep,
     // seeding) is stage 0, the main pass alone is stage 1
     if (ev) cudaEventRecord(ev[1], g->stream);
-    a.tile0_mul = tpc;
-    a.tile_step = 1;
+    // contiguous tile ranges per CTA; a compacted set's tiles are dealt
+    // round robin instead, so the rows that exist (a prefix of its tiles)
+    // spread over the CTAs
+    a.tile0_mul = rs ? 1 : tpc;
+    a.tile_step = rs ? (uint64_t)grow : 1;
     PV_CUDA_OK(run(a), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
     uint8_t *d_unc = (certify || num_cert) ? (uint8_t *)(c + off_unc) : nullptr;

@@ -9,8 +9,10 @@
 //    (from the posting rows), so a comparison or IN list is counted exactly
 //    by binary search, and AND / OR / NOT combine lower / upper bounds;
 //  * a batch whose queries share one filter bounded by a small count
-//    compacts that filter's bitmap into a row-id list on the device,
-//    computes the exact FP32 distance of every (query, listed row) and
+//    compacts that filter's bitmap into a row-id list on the device and
+//    either gathers those rows into a contiguous set for the tensor-core
+//    scan (2048+ rows, when the batch's mode scans on the tensor cores),
+//    or computes the exact FP32 distance of every (query, listed row) and
 //    selects each query's top-k from those keys (a radix select).
 // Results equal the full scan's: same rows, same FP32 distances.
 #include <math.h>
@@ -275,6 +277,93 @@ gather_dist_kernel(const float *__restrict__ vecs, int dpad, const float *__rest
         if (lane < GD_QT && q0 + lane < nq)
             keys[(uint64_t)(q0 + lane) * cap + r] = make_key(mine, row);
     }
+}
+
+// The listed rows in the tensor-core scan's operand layout: compacted row i
+// (i < min(*count, cap)) is index row ids[i] — its operand row (row_bytes,
+// a multiple of 16), norm and fp8 scale; one warp per row, 16-byte copies.
+// valid[w] marks the compacted rows [32w, 32w + 32) that exist.
+__global__ void __launch_bounds__(256)
+gather_rows_kernel(const unsigned char *__restrict__ src, size_t row_bytes,
+                   const float *__restrict__ norms, const float *__restrict__ scales,
+                   const uint32_t *__restrict__ ids, const unsigned long long *__restrict__ count,
+                   uint64_t cap, unsigned char *__restrict__ dst, float *__restrict__ dnorm,
+                   float *__restrict__ dscale, uint32_t *__restrict__ valid, uint64_t vwords) {
+    const uint64_t n = min((unsigned long long)cap, *count);
+    const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t w = gt; w < vwords; w += nthreads) {
+        const uint64_t r0 = w * 32;
+        valid[w] = r0 >= n ? 0u : n - r0 >= 32 ? 0xFFFFFFFFu : (1u << (n - r0)) - 1u;
+    }
+    const int lane = threadIdx.x & 31;
+    const size_t n16 = row_bytes / 16;
+    for (uint64_t i = gt >> 5; i < n; i += nthreads >> 5) {
+        const uint32_t r = __ldg(ids + i);
+        const uint4 *s4 = (const uint4 *)(src + (size_t)r * row_bytes);
+        uint4 *d4 = (uint4 *)(dst + (size_t)i * row_bytes);
+        for (size_t j = lane; j < n16; j += 32) d4[j] = __ldg(s4 + j);
+        if (lane == 0) {
+            dnorm[i] = __ldg(norms + r);
+            if (dscale) dscale[i] = __ldg(scales + r);
+        }
+    }
+}
+
+// The sparse route on the tensor cores: the filter's bitmap is compacted to
+// a row list, the listed rows are gathered into a contiguous set in the
+// scan's operand layout (the upload's BF16 / FP8 rows, or the f32 rows read
+// as TF32 for exact-mode batches), and the tensor-core scan runs over that
+// set with the same supersets, certificates and re-rank as over the whole
+// index; keys carry the index rows, so ties order as in the full scan.
+int sparse_tc_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, bool tf32,
+                     FvHit *d_out, uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev,
+                     char *errbuf, size_t errlen) {
+    const int nq = db.nq;
+    char *d = db.stage_d->as<char>();
+    const float *d_q = (const float *)(d + db.off_q);
+    const int32_t *d_qprog = (const int32_t *)(d + db.off_qprog);
+    const uint64_t bm_words = (g->count + 31) / 32;
+    ScanScratch &s = g->scan;
+    const bool fp8 = !tf32 && g->precision == FV_GPU_PREC_FP8;
+    const size_t row_bytes = tf32 ? (size_t)g->dpad * 4 : (size_t)g->kpad * (fp8 ? 1 : 2);
+    const uint64_t cap = std::max<uint64_t>(bound, 1);
+    const uint64_t cap_pad = (cap + 127) & ~127ull;  // whole 128-row tiles
+    const uint64_t vwords = cap_pad / 32;
+    // scratch: [count u64][ids u32 x cap_pad][rows][norms][scales][valid words]
+    auto al = [](size_t x, size_t a) { return (x + a - 1) & ~(a - 1); };
+    const size_t off_ids = 256;
+    const size_t off_rows = al(off_ids + cap_pad * 4, 1024);
+    const size_t off_norm = al(off_rows + cap_pad * row_bytes, 1024);
+    const size_t off_scale = al(off_norm + cap_pad * 4, 256);
+    const size_t off_valid = al(off_scale + (fp8 ? cap_pad * 4 : 0), 256);
+    PV_CUDA_OK(s.sparse.ensure(off_valid + vwords * 4 + 256), errbuf, errlen);
+    char *sp = s.sparse.as<char>();
+    unsigned long long *d_count = (unsigned long long *)sp;
+    uint32_t *ids = (uint32_t *)(sp + off_ids);
+    unsigned char *rows = (unsigned char *)(sp + off_rows);
+    float *norms = (float *)(sp + off_norm);
+    float *scales = fp8 ? (float *)(sp + off_scale) : nullptr;
+    uint32_t *valid = (uint32_t *)(sp + off_valid);
+    PV_CUDA_OK(cudaMemsetAsync(d_count, 0, 8, g->stream), errbuf, errlen);
+    unsigned blocks = (unsigned)std::min<uint64_t>((bm_words + 255) / 256, (uint64_t)g->sm_count * 4);
+    if (!blocks) blocks = 1;
+    compact_kernel<<<blocks, 256, 0, g->stream>>>(s.bitmaps.as<uint32_t>(), bm_words, g->count,
+                                                  ids, d_count, cap);
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    const unsigned gblocks = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((cap + 7) / 8, (uint64_t)g->sm_count * 8));
+    const unsigned char *src = tf32 ? (const unsigned char *)g->d_vecs
+                                    : (const unsigned char *)g->d_vlow;
+    gather_rows_kernel<<<gblocks, 256, 0, g->stream>>>(
+        src, row_bytes, tf32 ? g->d_norm32 : g->d_norm, fp8 ? g->d_vscale : nullptr, ids, d_count,
+        cap, rows, norms, scales, valid, vwords);
+    PV_CUDA_OK(cudaGetLastError(), errbuf, errlen);
+    g->launches += 2;  // compaction, gather
+    const TcRowSet rs{rows, norms, scales, cap_pad, ids, d_count};
+    return launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, valid, vwords,
+                          s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
+                          errbuf, errlen, nullptr, tf32, &rs);
 }
 
 // The sparse route of brute_launch: every query uses program 0, whose

@@ -15,7 +15,7 @@
 //
 // Warp roles (64 + 128 * EPI threads): warp 0 TMA producer, warp 1 MMA
 // issuer, then EPI groups of 4 epilogue warps (warp w reads TMEM lanes
-// 32*(w%4).. ; group h takes its share of each tile's rows). A batch of at
+// 32*(w%4).. ; group h owns the tiles h, h + EPI, ...). A batch of at
 // most 64 (32) queries is replicated 2 (4) times down the 128 query slots.
 // All waits are bounded by a deadline and unwind through an abort flag.
 #pragma once
@@ -44,7 +44,9 @@ constexpr int TC_MAX_SUPERSET = 1024;
 constexpr int TC_MAX_LIST = 64;
 constexpr int TC_MAX_STAGES = 8;   // TMA pipeline stages at most
 constexpr int TC_NR = 8;            // tiles of row norms in flight (shared-memory ring)
-constexpr int TC_NSLOT_F = 2 * TC_BN;  // floats per norm slot: norms, then fp8 scales
+// words per norm slot: norms, fp8 scales, then the index rows of a
+// compacted row set (each part one tile's 128 entries)
+constexpr int TC_NSLOT_F = 3 * TC_BN;
 // TMEM accumulators (128 columns each, all 512 of the SM's): the MMA of a
 // tile waits only for the epilogue of the tile NACC back, so the MMA's own
 // latency (issue to completion ~1 us for a BF16 tile) overlaps up to three
@@ -100,6 +102,11 @@ struct TcArgs {
     int nconsts;
     const double *__restrict__ cols;
     int ncols;
+    // rows scanned are a compacted set: scanned row i is index row rowids[i]
+    // (padded to whole tiles; keys carry the index row), of which the first
+    // *nrows_dev exist (tiles past them are skipped); null: the index's rows
+    const uint32_t *__restrict__ rowids;
+    const unsigned long long *nrows_dev;
     unsigned long long *tau;  // [nq] grid-wide bound
     // kept keys: each list appends its best kwrite keys to its query's dense
     // run dense[q][0 .. dcnt[q]) (any order; dcap >= lists per query * kwrite)
@@ -171,11 +178,11 @@ __device__ __forceinline__ void tc_init_barriers(const TcSmem &m, int NS, int EP
     }
     for (int i = 0; i < TC_NACC; i++) {
         mbar_init(&m.tfull[i], 1);
-        mbar_init(&m.tempty[i], TC_BM * EPI);
+        mbar_init(&m.tempty[i], TC_BM);  // the epilogue group that owns the tile
     }
     for (int i = 0; i < TC_NR; i++) {
         mbar_init(&m.nfull[i], 1);
-        mbar_init(&m.nempty[i], 4 * EPI);  // one arrival per epilogue warp
+        mbar_init(&m.nempty[i], 4);  // one arrival per warp of the owning group
     }
     mbar_init(m.qbar, 1);
     mbar_init(m.done, 1);
@@ -218,7 +225,12 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // this CTA's tiles: tile0 + t * tile_step, t < ntiles
     const uint64_t tile0 = (uint64_t)rgrp * a.tile0_mul;
-    const uint64_t ntiles_all = (a.nrows + TC_BN - 1) / TC_BN;
+    uint64_t nrows_eff = a.nrows;
+    if (a.nrows_dev) {
+        const unsigned long long nd = *a.nrows_dev;
+        if (nd < nrows_eff) nrows_eff = nd;
+    }
+    const uint64_t ntiles_all = (nrows_eff + TC_BN - 1) / TC_BN;
     uint64_t ntiles =
         tile0 < ntiles_all ? (ntiles_all - tile0 + a.tile_step - 1) / a.tile_step : 0;
     if (ntiles > a.tiles_per_cta) ntiles = a.tiles_per_cta;
@@ -236,7 +248,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             for (int kb = 0; kb < KBt; kb++)
                 tma_load_2d(sQ + (size_t)kb * TC_BOX, &tmQ, kb * BOXE,
                             qtile * TC_BM, qbar);
-            const uint32_t nbytes = (FP8 ? 2 : 1) * TC_BN * 4;
+            const uint32_t nbytes = ((FP8 ? 2 : 1) + (a.rowids ? 1 : 0)) * TC_BN * 4;
             uint64_t it = it0, nt = T0;  // stages and norm slots issued (running)
             bool ok = true;
             for (uint64_t t = 0; t < ntiles && ok; t++) {
@@ -256,6 +268,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                     float *dst = snorm + (size_t)ns * TC_NSLOT_F;
                     bulk_load(dst, a.xnorm + tile * TC_BN, TC_BN * 4, &nfull[ns]);
                     if (FP8) bulk_load(dst + TC_BN, a.xscale + tile * TC_BN, TC_BN * 4, &nfull[ns]);
+                    if (a.rowids)
+                        bulk_load(dst + 2 * TC_BN, a.rowids + tile * TC_BN, TC_BN * 4, &nfull[ns]);
                     nt = T + 1;
                 }
                 for (int kc = 0; kc < nkc; kc++, it++) {
@@ -332,10 +346,12 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
         }
     } else {
         // ------------------------------------------------ epilogue
-        // EPI warps per TMEM lane quadrant: warp w serves the query slots of
-        // lanes 32*(w%4).. (replica m / bq of query m % bq) and, of every
-        // tile, the CW rows of part (half, replica).
-        constexpr int CPH = 4 / EPI;         // 32-row chunks per half at most
+        // EPI groups of 4 warps; warp w serves the query slots of TMEM lanes
+        // 32*(w%4).. (replica m / bq of query m % bq). Group h owns the tiles
+        // whose running number T has T % EPI == h, so each group pays a
+        // tile's fixed costs (barrier waits, word loads, arrivals) once per
+        // EPI tiles, and takes the CW rows of its replica from each of them.
+        constexpr int CPH = TC_BN / 32;      // 32-row chunks per part at most
         constexpr int NSLOT = TC_BM * EPI;   // list / stage slots
         const int qd = warp & 3;
         const int half = (warp - 2) >> 2;
@@ -343,9 +359,9 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
         const int rp = m / a.bq;             // replica (uniform within a warp)
         const int slot = half * TC_BM + m;
         const int qg = qtile * TC_BM + (m - rp * a.bq);
-        const int CW = TC_BN / (EPI * a.rep);  // rows of a tile per part (>= 32)
+        const int CW = TC_BN / a.rep;  // rows of a tile per replica (>= 32)
         const int nch = CW / 32;
-        const int col0 = (half * a.rep + rp) * CW;
+        const int col0 = rp * CW;
         const bool qvalid = qg < a.nq;
         const float qn = qvalid ? a.qnorm[qg] : 0.f;
         const float qs = (FP8 && qvalid) ? a.qscale[qg] : 1.f;
@@ -434,7 +450,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
         // one tile: false when a wait gave up
         auto tile_body = [&](uint64_t t, const uint32_t (&bw)[CPH], unsigned long long gt,
                              uint32_t (&nbw)[CPH], unsigned long long &ngt) -> bool {
-            if (t + 1 < ntiles) load_words(t + 1, nbw, ngt);
+            if (t + EPI < ntiles) load_words(t + EPI, nbw, ngt);
             const uint64_t T = T0 + t;  // running tile count: barrier phases
             const int acc = (int)(T % TC_NACC);
             const uint32_t aph = (uint32_t)((T / TC_NACC) & 1);
@@ -449,18 +465,13 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             const uint64_t rbase = (tile0 + t * a.tile_step) * TC_BN + col0;
             const float *xnv = snorm + (size_t)ns * TC_NSLOT_F + col0;
             const float *xsv = xnv + TC_BN;
+            const uint32_t *ridv = (const uint32_t *)(xnv + 2 * TC_BN);
             if (gt < thr) {
                 thr = gt;
                 thr_d = key_dist(gt);
             }
-#pragma unroll
-            for (int c = 0; c < CPH; c++) {
-                if (c >= nch) break;
-                uint32_t r[32];
-                tmem_ld_32x32b_x32(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)acc * TC_BN +
-                                       col0 + c * 32,
-                                   r);
-                tmem_ld_wait();
+            // one 32-row chunk of the tile, its accumulator columns in r
+            auto chunk = [&](const int c, const uint32_t(&r)[32]) {
                 // hot loop: distances and a candidate mask only; the rare
                 // admissions run below, outside the unrolled code (a negative
                 // norm-form value is clamped there)
@@ -491,7 +502,8 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                     cmask &= cmask - 1;
                     const float d = fmaxf(stage[i * NSLOT + slot], 0.f);
                     const uint64_t row = rbase + c * 32 + i;
-                    const uint64_t key = make_key(d, (uint32_t)row);
+                    const uint32_t rid = a.rowids ? ridv[c * 32 + i] : (uint32_t)row;
+                    const uint64_t key = make_key(d, rid);
                     // <= : the seeded bound is itself a row key that this
                     // pass must admit again (keys are unique)
                     if (key > thr) continue;
@@ -534,6 +546,18 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                         thr_d = key_dist(lmax);
                     }
                 }
+            };
+            // (loading two chunks before one wait measured slower: 0.0644 vs
+            // 0.0615 ms for the BF16 pass at batch 64)
+            const uint32_t tbase =
+                tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)acc * TC_BN + col0;
+#pragma unroll
+            for (int c = 0; c < CPH; c++) {
+                if (c >= nch) break;
+                uint32_t r0[32];
+                tmem_ld_32x32b_x32(tbase + c * 32, r0);
+                tmem_ld_wait();
+                chunk(c, r0);
             }
             tc_fence_before();
             mbar_arrive(&tempty[acc]);
@@ -550,10 +574,12 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
         };
         uint32_t wA[CPH], wB[CPH];
         unsigned long long gA = KEY_MAX, gB = KEY_MAX;
-        if (ntiles) load_words(0, wA, gA);
-        for (uint64_t t = 0; t < ntiles; t += 2) {
+        // this group's first tile of the pass
+        const uint64_t tfirst = (uint64_t)((half - (int)(T0 % EPI) + EPI) % EPI);
+        if (tfirst < ntiles) load_words(tfirst, wA, gA);
+        for (uint64_t t = tfirst; t < ntiles; t += 2 * EPI) {
             if (!tile_body(t, wA, gA, wB, gB)) { ok = false; break; }
-            if (t + 1 < ntiles && !tile_body(t + 1, wB, gB, wA, gA)) { ok = false; break; }
+            if (t + EPI < ntiles && !tile_body(t + EPI, wB, gB, wA, gA)) { ok = false; break; }
         }
         if (!ok) {
             *abort_flag = 1;

@@ -117,6 +117,10 @@ def test_fp8_large_k_superset_certified_or_rerun(clustered):
                            kind="stable")
         vecs, cols = np.ascontiguousarray(vecs[order]), np.ascontiguousarray(cols[:, order])
     gi = GpuIndex(vecs, cols, precision=FV_GPU_PREC_FP8)
+    # one epilogue group, no query replicas: each list then sees all 128 rows
+    # of its CTA's tiles (512 rows), more than its 64 keys (with replicas a
+    # list can see as few rows as it holds, and never drop one)
+    assert _lib.lib().pv_tc_shape(gi.handle, 1, 0, 0, 1, 0) == 0
     preds = [None, datagen.six_predicates()["sel70%"]] * 16
     bp = pred.concat(preds, 20000)
     ids, dists, cnt, _ = gi.brute_batch_raw(ds.queries, bp, 100)
