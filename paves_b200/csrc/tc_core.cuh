@@ -148,8 +148,8 @@ __device__ __forceinline__ TcSmem tc_carve(unsigned char *base, int KBt, int NS,
     // per (query, part) lists [KP][128*EPI] and candidate staging [32][128*EPI]
     m.lists = (uint64_t *)(m.sX + (size_t)NS * m.SB);
     m.stage = (float *)(m.lists + (size_t)TC_BM * EPI * KPcap);
-    // row norms (and fp8 scales) of a tile, TC_NR tiles in flight (slot =
-    // [norms 128][scales 128])
+    // row norms (and fp8 scales, compacted-set row ids) of a tile, TC_NR
+    // tiles in flight (slot = [norms 128][scales 128][row ids 128])
     m.snorm = m.stage + 32 * TC_BM * EPI;
     uint64_t *bars = (uint64_t *)(m.snorm + (size_t)TC_NR * TC_NSLOT_F);
     m.full = bars;              // [NS]
@@ -496,6 +496,35 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                     }
                 }
                 cmask &= bw[c];
+                // warm-up: an empty list facing more than KP candidates (a
+                // pass without a bound: the first chunk of a compacted set,
+                // of a seeding pass) admits only the chunk's KP best - the
+                // KP-th smallest distance becomes the admission bound -
+                // instead of inserting every candidate into its heap one by
+                // one (the bound: ascending distinct values, counting ties)
+                if (!lazy && n == 0 && __popc(cmask) > KP) {
+                    float v[32];
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        v[i] = ((cmask >> i) & 1u) ? fmaxf(stage[i * NSLOT + slot], 0.f)
+                                                   : __int_as_float(0x7f800000);
+                    float kth = -1.f;
+                    for (int cnt = 0; cnt < KP;) {
+                        float m = __int_as_float(0x7f800000);
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                            if (v[i] > kth) m = fminf(m, v[i]);
+                        int c2 = 0;
+#pragma unroll
+                        for (int i = 0; i < 32; i++) c2 += v[i] == m ? 1 : 0;
+                        kth = m;
+                        cnt += c2;
+                    }
+                    if (kth < thr_d) thr_d = kth;
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        if (v[i] > thr_d) cmask &= ~(1u << i);
+                }
 #pragma unroll 1
                 while (cmask) {
                     const int i = __ffs(cmask) - 1;
