@@ -133,8 +133,12 @@ constexpr double PV_LAZY_MIN_PASS = 0.125;
 // Sparse batches whose filter matches at least this many rows (bounded on
 // the host) scan their compacted rows on the tensor cores when the batch's
 // mode can (sparse_tc_launch); smaller ones compute every listed row's
-// exact distance on the CUDA cores (sparse_launch).
-constexpr uint64_t PV_SPARSE_TC_MIN_ROWS = 2048;
+// exact distance on the CUDA cores (sparse_launch). Measured at batch 64
+// over 1M rows: at a bound of 10,000 rows both routes took 0.078 ms (1 %
+// filter), at ~1,000 matching rows the CUDA-core route was faster (0.040
+// vs 0.064 ms); a compacted pass pays its warm-up admissions on every
+// tile, since it has too few tiles for a seeding pass.
+constexpr uint64_t PV_SPARSE_TC_MIN_ROWS = 16384;
 int sparse_tc_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, uint64_t bound, bool tf32,
                      FvHit *d_out, uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev,
                      char *errbuf, size_t errlen);

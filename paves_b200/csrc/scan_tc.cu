@@ -46,7 +46,7 @@ namespace pv {
 
 using namespace sm100;
 
-template <int KIND, int EPI>
+template <int KIND, int EPI, bool WARM>
 __global__ void __launch_bounds__(64 + 128 * EPI, 1)
 scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmQ,
                TcArgs a) {
@@ -70,7 +70,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     pdl_wait();  // the previous kernel's outputs (query tile, bounds, bitmaps)
     pdl_trigger();
     TcRun run;
-    tc_pass<KIND, EPI>(&tmX, &tmQ, a, sm, s_tmem, run, &s_abort, blockIdx.x % a.qtiles,
+    tc_pass<KIND, EPI, WARM>(&tmX, &tmQ, a, sm, s_tmem, run, &s_abort, blockIdx.x % a.qtiles,
                       blockIdx.x / a.qtiles);
     if (warp == 1) {
         tc_fence_after();
@@ -267,21 +267,21 @@ bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
     return tc_smem(g->kpad * esz / TC_KB_BYTES, ns, KP, epi) <= 227 * 1024;
 }
 
-template <int KIND, int EPI>
+template <int KIND, int EPI, bool WARM>
 static cudaError_t tc_launch_kind(int grid, size_t smem, cudaStream_t st, const CUtensorMap &tmX,
                                   const CUtensorMap &tmQ, const TcArgs &a) {
-    cudaError_t e = raise_smem_limit((const void *)scan_tc_kernel<KIND, EPI>, smem);
+    cudaError_t e = raise_smem_limit((const void *)scan_tc_kernel<KIND, EPI, WARM>, smem);
     if (e != cudaSuccess) return e;
-    return launch_pdl(scan_tc_kernel<KIND, EPI>, dim3(grid), dim3(64 + 128 * EPI), smem, st, tmX,
-                      tmQ, a);
+    return launch_pdl(scan_tc_kernel<KIND, EPI, WARM>, dim3(grid), dim3(64 + 128 * EPI), smem,
+                      st, tmX, tmQ, a);
 }
 
-template <int EPI>
+template <int EPI, bool WARM>
 static cudaError_t tc_launch(int kind, int grid, size_t smem, cudaStream_t st,
                             const CUtensorMap &tmX, const CUtensorMap &tmQ, const TcArgs &a) {
-    if (kind == TCK_FP8) return tc_launch_kind<TCK_FP8, EPI>(grid, smem, st, tmX, tmQ, a);
-    if (kind == TCK_TF32) return tc_launch_kind<TCK_TF32, EPI>(grid, smem, st, tmX, tmQ, a);
-    return tc_launch_kind<TCK_BF16, EPI>(grid, smem, st, tmX, tmQ, a);
+    if (kind == TCK_FP8) return tc_launch_kind<TCK_FP8, EPI, WARM>(grid, smem, st, tmX, tmQ, a);
+    if (kind == TCK_TF32) return tc_launch_kind<TCK_TF32, EPI, WARM>(grid, smem, st, tmX, tmQ, a);
+    return tc_launch_kind<TCK_BF16, EPI, WARM>(grid, smem, st, tmX, tmQ, a);
 }
 
 // Launches query prep, the tensor-core scan, the per-query merge and the
@@ -478,9 +478,14 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
             a.trace_tiles = 64;
         }
     }
-    auto run = [&](const TcArgs &args) {
-        return EPI == 2 ? tc_launch<2>(kind, args.grow * qtiles, smem, g->stream, tmX, tmQ, args)
-                        : tc_launch<1>(kind, args.grow * qtiles, smem, g->stream, tmX, tmQ, args);
+    // warm: a pass that starts without a bound (see tc_pass)
+    auto run = [&](const TcArgs &args, bool warm) {
+        const int gr = args.grow * qtiles;
+        if (EPI == 2)
+            return warm ? tc_launch<2, true>(kind, gr, smem, g->stream, tmX, tmQ, args)
+                        : tc_launch<2, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
+        return warm ? tc_launch<1, true>(kind, gr, smem, g->stream, tmX, tmQ, args)
+                    : tc_launch<1, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);
@@ -513,7 +518,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         sa.push_tau = sa.KP == S ? 1 : 0;
         sa.fullmin = nullptr;
         g->launches += 2;  // seeding pass + its merge
-        PV_CUDA_OK(run(sa), errbuf, errlen);
+        PV_CUDA_OK(run(sa, true), errbuf, errlen);
         // the merge leaves the counts at zero for the main pass
         PV_CUDA_OK(launch_dense_merge(a.dense, dcap, d_dcnt, true, nullptr, a.tau, S, d_qprog,
                                       popcnt, g->count, nq, cand, ccnt,
@@ -528,7 +533,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     // spread over the CTAs
     a.tile0_mul = rs ? 1 : tpc;
     a.tile_step = rs ? (uint64_t)grow : 1;
-    PV_CUDA_OK(run(a), errbuf, errlen);
+    PV_CUDA_OK(run(a, rs != nullptr), errbuf, errlen);
     if (ev) cudaEventRecord(ev[2], g->stream);
     uint8_t *d_unc = (certify || num_cert) ? (uint8_t *)(c + off_unc) : nullptr;
     if (S == (int)topb) {

@@ -202,7 +202,10 @@ struct TcRun {
 // tiles and passes, so a kernel can run several passes over the same
 // barriers and tensor memory (every role advances the counts alike).
 // Returns false when a wait of this CTA gave up (*abort_flag set).
-template <int KIND, int EPI>
+// WARM: compile the warm-up admission bound (passes that start without a
+// bound: seeding passes, compacted sets; it costs the main pass over the
+// whole index ~7 % in registers and code for nothing, so that one omits it)
+template <int KIND, int EPI, bool WARM = false>
 __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorMap *tmQp,
                                         const TcArgs &a, const TcSmem &sm, uint32_t tmem,
                                         TcRun &run, volatile int *abort_flag, int qtile,
@@ -502,7 +505,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                 // KP-th smallest distance becomes the admission bound -
                 // instead of inserting every candidate into its heap one by
                 // one (the bound: ascending distinct values, counting ties)
-                if (!lazy && n == 0 && __popc(cmask) > KP) {
+                if (WARM && !lazy && n == 0 && __popc(cmask) > KP) {
                     float v[32];
 #pragma unroll
                     for (int i = 0; i < 32; i++)

@@ -1,5 +1,5 @@
 """The sparse route on the tensor cores: a batch whose queries share one
-selective filter (bounded on the host at 2048+ matching rows) compacts the
+selective filter (bounded on the host at 16384+ matching rows) compacts the
 matching rows and scans only them on the tensor cores (BF16 / FP8 rows, or
 the f32 rows read as TF32 in the exact mode).
 
@@ -14,16 +14,16 @@ from oracle import cpu
 from paves_b200 import (FV_GPU_PREC_BF16, FV_GPU_PREC_FP8, GpuIndex, _lib, datagen, pred)
 
 pytestmark = pytest.mark.gpu
-N, D = 300_007, 128
+N, D = 1_000_003, 128
 P, Cc = datagen.COL_PRICE, datagen.COL_CATEGORY
 
 FILTERS = {
-    # ~1 % of rows (price is uniform in [0, 1000)): ~3000 rows
-    "price<10": pred.Cmp(P, "<", 10.0),
-    # ~0.6 %, two columns (bounded by the price term: ~6000 rows)
-    "price<20&cat3-5": pred.And(pred.Cmp(P, "<", 20.0), pred.In(Cc, [3.0, 4.0, 5.0])),
-    # ~4 %: ~12000 rows, still under the route's limit (rows / 16)
-    "price<40": pred.Cmp(P, "<", 40.0),
+    # ~2 % of rows (price is uniform in [0, 1000)): ~20,000 rows
+    "price<20": pred.Cmp(P, "<", 20.0),
+    # ~1.2 %, two columns (bounded by the price term: ~40,000 rows)
+    "price<40&cat3-5": pred.And(pred.Cmp(P, "<", 40.0), pred.In(Cc, [3.0, 4.0, 5.0])),
+    # ~5 %: ~50,000 rows, still under the route's limit (rows / 16)
+    "price<50": pred.Cmp(P, "<", 50.0),
     # ~0.3 %: below the tensor-core threshold, the CUDA-core sparse route
     "price<3": pred.Cmp(P, "<", 3.0),
 }
@@ -47,26 +47,36 @@ def _exact(ds, gi, q, p, topb):
         assert trunc[i] == (o_pass[i] > topb), i
 
 
+@pytest.fixture(scope="module")
+def bf16(ds):
+    gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_BF16)
+    yield gi
+    gi.close()
+
+
+@pytest.fixture(scope="module")
+def fp32(ds):
+    gi = GpuIndex(ds.vectors, ds.cols)
+    yield gi
+    gi.close()
+
+
 @pytest.mark.parametrize("name", list(FILTERS))
 @pytest.mark.parametrize("topb", [10, 100])
-def test_bf16_sparse_matches_oracle(ds, name, topb):
-    gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_BF16)
-    _exact(ds, gi, ds.queries, FILTERS[name], topb)
-    gi.close()
+def test_bf16_sparse_matches_oracle(ds, bf16, name, topb):
+    _exact(ds, bf16, ds.queries, FILTERS[name], topb)
 
 
 @pytest.mark.parametrize("name", list(FILTERS))
-def test_fp32_exact_sparse_matches_oracle(ds, name):
-    gi = GpuIndex(ds.vectors, ds.cols)
-    _exact(ds, gi, ds.queries[:32], FILTERS[name], 10)
+def test_fp32_exact_sparse_matches_oracle(ds, fp32, name):
+    _exact(ds, fp32, ds.queries[:32], FILTERS[name], 10)
     if name != "price<3":
-        assert _lib.lib().pv_last_exact_tc(gi.handle) == 1
-    gi.close()
+        assert _lib.lib().pv_last_exact_tc(fp32.handle) == 1
 
 
 def test_fp8_sparse_recall(ds):
     gi = GpuIndex(ds.vectors, ds.cols, precision=FV_GPU_PREC_FP8)
-    p = FILTERS["price<10"]
+    p = FILTERS["price<20"]
     bp = pred.concat([p] * 64, N)
     ids, dists, cnt, _ = gi.brute_batch_raw(ds.queries, bp, 10)
     assert _lib.lib().pv_last_sparse(gi.handle) == 1
@@ -89,7 +99,7 @@ def test_non_integer_rows_exact_mode(ds):
     vecs = (ds.vectors + rng.standard_normal(ds.vectors.shape) * 0.37).astype(np.float32)
     qs = (ds.queries[:32] + rng.standard_normal((32, D)) * 0.37).astype(np.float32)
     gi = GpuIndex(vecs, ds.cols)
-    p = FILTERS["price<20&cat3-5"]
+    p = FILTERS["price<40&cat3-5"]
     bp = pred.concat([p] * 32, N)
     ids, dists, cnt, _ = gi.brute_batch_raw(qs, bp, 10)
     assert _lib.lib().pv_last_sparse(gi.handle) == 1
