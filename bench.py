@@ -879,7 +879,8 @@ def main():
             ms_tot += sum(st)
             if L.pv_last_exact_tc(gi.handle):
                 on_tc += 1
-                scan_tc_ms.append(st[1] / per_class)
+                if not L.pv_last_sparse(gi.handle):  # a pass over the whole index
+                    scan_tc_ms.append(st[1] / per_class)
             bxs.append(bx)
         ans = [fetch(bx, BATCH, TOPK) for bx in bxs]
         for bx in bxs:
