@@ -331,7 +331,7 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
     const size_t off_tr = off_cnt + al256((size_t)nq * 4);
     const size_t obytes = off_tr + al256((size_t)nq);
     PV_CUDA_OK(g->scan.out_d.ensure(obytes), errbuf, errlen);
-    PV_CUDA_OK(g->scan.out_h.ensure(obytes), errbuf, errlen);
+    PV_CUDA_OK(g->scan.out_h.ensure(obytes + 256), errbuf, errlen);  // + the watchdog word
     char *od = g->scan.out_d.as<char>();
     if (brute_upload(g, db, errbuf, errlen)) return -1;
     cudaEventRecord(g->ev0, g->stream);
@@ -341,6 +341,7 @@ int brute_run_host(FvGpuIndex *g, int nq, const float *queries, const PredBatch 
     cudaEventRecord(g->ev1, g->stream);
     PV_CUDA_OK(cudaMemcpyAsync(g->scan.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream),
                errbuf, errlen);
+    tc_watchdog_enqueue(g, (int *)(g->scan.out_h.as<char>() + obytes));
     PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
     if (check_tc_watchdog(g, errbuf, errlen)) return -1;
     cudaEventElapsedTime(&g->last_kernel_ms, g->ev0, g->ev1);

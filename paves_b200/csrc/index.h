@@ -115,6 +115,7 @@ struct FvGpuIndex {
     pv::ScanScratch scan;
     pv::GraphScratch graph;
     int *tc_err = nullptr;  // watchdog word of the last tensor-core scan (device)
+    int *tc_err_h = nullptr;  // its copy in pinned memory, queued with the results
     uint8_t *tc_unc = nullptr;  // per query: superset not certified (last TC scan)
     int tc_unc_n = 0;
     int last_uncertain = 0;  // queries of the last call re-run exactly (or flagged)

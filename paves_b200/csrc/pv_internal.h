@@ -198,6 +198,9 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);
+// Queues the watchdog word's copy into pinned h_word on g's stream (after
+// the results' copy); the next check_tc_watchdog reads it there.
+void tc_watchdog_enqueue(FvGpuIndex *g, int *h_word);
 
 // ---- HNSW sections (hnsw_build.cpp) for the GPU builder (hnsw_gpu.cu)
 }  // namespace pv

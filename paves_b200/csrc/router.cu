@@ -1178,6 +1178,8 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
             return -1;
         RT_OK(cudaEventRecord(ev[3], g->stream));
         RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
+        // the watchdog word rides behind the results (the spare tail of out_h)
+        tc_watchdog_enqueue(g, (int *)(s.out_h.as<char>() + obytes - 64));
     }
     RT_OK(cudaEventSynchronize(ev[2]));
     // each query takes the route the router chose for it: the graph search

@@ -566,6 +566,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     g->tc_unc_n = nq;
     if (ev) cudaEventRecord(ev[3], g->stream);
     g->tc_err = d_err;
+    g->tc_err_h = nullptr;  // its host copy, if any, is queued by the caller
     if (tracing && d_trace) {
         uint64_t h[64 * 4];
         cudaStreamSynchronize(g->stream);
@@ -582,12 +583,29 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
 }  // namespace pv
 
 namespace pv {
+// Queues the copy of the watchdog word into pinned host memory behind the
+// batch's own result copy, so reading it costs no extra round trip.
+void tc_watchdog_enqueue(FvGpuIndex *g, int *h_word) {
+    g->tc_err_h = nullptr;
+    if (!g->tc_err) return;
+    if (cudaMemcpyAsync(h_word, g->tc_err, 4, cudaMemcpyDeviceToHost, g->stream) == cudaSuccess)
+        g->tc_err_h = h_word;
+    else
+        (void)cudaGetLastError();
+}
+
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen) {
     if (!g->tc_err) return 0;
     int e = 0;
-    PV_CUDA_OK(cudaMemcpyAsync(&e, g->tc_err, 4, cudaMemcpyDeviceToHost, g->stream), errbuf,
-               errlen);
-    PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    if (g->tc_err_h) {  // queued with the results
+        PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+        e = *(volatile int *)g->tc_err_h;
+        g->tc_err_h = nullptr;
+    } else {
+        PV_CUDA_OK(cudaMemcpyAsync(&e, g->tc_err, 4, cudaMemcpyDeviceToHost, g->stream), errbuf,
+                   errlen);
+        PV_CUDA_OK(cudaStreamSynchronize(g->stream), errbuf, errlen);
+    }
     if (e) {
         cudaMemsetAsync(g->tc_err, 0, 4, g->stream);
         snprintf(errbuf, errlen, "gpu: tensor-core scan wait expired (role %d)", e);
