@@ -847,97 +847,64 @@ __global__ void router_decide_kernel(const float *__restrict__ Z3, int nq,
 // batch call (the first beside the bitmaps, the second beside the start of
 // the search). Same features, network and
 // decision rule as router_features_kernel -> mlp_infer_kernel ->
-// router_decide_kernel; the centroid distances are summed in another order
-// (lanes over dimensions, then a shuffle tree), so feature values may
-// differ from those kernels' in the last bits.
+// router_decide_kernel (the centroid distances summed in the same order,
+// so the features are the same values).
 //
-// Step 1: CTA (chunk, query) scores centroid chunk `chunk` (RT_CHUNKS of
-// them) for its query with 4 warps, four centroids per warp at a time, and
-// writes the chunk's 8 smallest squared distances to part[q][chunk][8].
-constexpr int RT_CHUNKS = 8;
+// Step 1: squared distances of every (query, centroid) pair, dist[q][c],
+// summed over the dimensions in order, four at a time - the order of
+// router_features_kernel, so the features equal the training ones. A CTA
+// takes a tile of 64 queries x 32 centroids through shared memory (rows
+// padded by one word: the 32 centroid rows a warp reads fall in 32
+// banks), 64 dimensions at a time; each thread owns 4 queries x 2
+// centroids.
+constexpr int RT_TQ = 64, RT_TC = 32, RT_TD = 64;
 
-__global__ void __launch_bounds__(128) router_cent_kernel(const float *__restrict__ queries,
-                                                          int dpad,
+__global__ void __launch_bounds__(256) router_cent_kernel(const float *__restrict__ queries,
+                                                          int nq, int dpad,
                                                           const float *__restrict__ cent,
-                                                          int ncent, float *__restrict__ part) {
-    __shared__ float cand[4][8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = blockIdx.y, chunk = blockIdx.x;
-    const int per = (ncent + RT_CHUNKS - 1) / RT_CHUNKS;
-    const int cb = chunk * per, ce = min(ncent, cb + per);
-    const float *qv = queries + (uint64_t)q * dpad;
-    float top[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) top[i] = INFINITY;
-    int mine_i = 0;  // the warp's centroids scored so far; lane mine_i % 32 keeps each
-    for (int c0 = cb + warp; c0 < ce; c0 += 16) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int j = lane * 4; j < dpad; j += 128) {
-            const float4 u = *(const float4 *)(qv + j);
+                                                          int ncent, float *__restrict__ dist) {
+    __shared__ float sq[RT_TQ][RT_TD + 1];
+    __shared__ float sc[RT_TC][RT_TD + 1];
+    const int tid = threadIdx.x;
+    const int c0 = blockIdx.x * RT_TC, q0 = blockIdx.y * RT_TQ;
+    const int tq = (tid >> 4) * 4, tc = (tid & 15) * 2;
+    float acc[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    for (int d0 = 0; d0 < dpad; d0 += RT_TD) {
+        const int dn = min(RT_TD, dpad - d0);
+        __syncthreads();
+        for (int i = tid; i < RT_TQ * RT_TD; i += 256) {
+            const int r = i / RT_TD, j = i - r * RT_TD;
+            sq[r][j] = (q0 + r < nq && j < dn) ? queries[(uint64_t)(q0 + r) * dpad + d0 + j] : 0.f;
+        }
+        for (int i = tid; i < RT_TC * RT_TD; i += 256) {
+            const int r = i / RT_TD, j = i - r * RT_TD;
+            sc[r][j] = (c0 + r < ncent && j < dn) ? cent[(uint64_t)(c0 + r) * dpad + d0 + j] : 0.f;
+        }
+        __syncthreads();
+        for (int j = 0; j < dn; j++) {
+            const float x0 = sc[tc][j], x1 = sc[tc + 1][j];
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const int c = c0 + 4 * k;
-                if (c >= ce) break;
-                const float4 v = __ldg((const float4 *)(cent + (uint64_t)c * dpad + j));
-                const float d0 = v.x - u.x, d1 = v.y - u.y, d2 = v.z - u.z, d3 = v.w - u.w;
-                acc[k] = fmaf(d0, d0, acc[k]);
-                acc[k] = fmaf(d1, d1, acc[k]);
-                acc[k] = fmaf(d2, d2, acc[k]);
-                acc[k] = fmaf(d3, d3, acc[k]);
+                const float u = sq[tq + k][j];
+                const float e0 = x0 - u, e1 = x1 - u;
+                acc[k][0] = fmaf(e0, e0, acc[k][0]);
+                acc[k][1] = fmaf(e1, e1, acc[k][1]);
             }
         }
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-#pragma unroll
-            for (int o = 16; o; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (c0 + 4 * k >= ce) break;
-            if (lane == (mine_i & 31) && acc[k] < top[7]) {
-                float v = acc[k];
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const float t = top[i];
-                    const bool sw = v < t;
-                    top[i] = sw ? v : t;
-                    v = sw ? t : v;
-                }
-            }
-            mine_i++;
-        }
     }
-    {
-        int head = 0;
-        float mine = INFINITY;
-        for (int r = 0; r < 8; r++) {
-            float best = head < 8 ? pick8(top, head) : INFINITY;
-            int who = lane;
-            warp_argmin(best, who);
-            if (lane == who) head++;
-            if (lane == r) mine = best;
-        }
-        if (lane < 8) cand[warp][lane] = mine;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        float v = cand[lane >> 3][lane & 7];
-        float out = INFINITY;
-        for (int r = 0; r < 8; r++) {
-            float best = v;
-            int who = lane;
-            warp_argmin(best, who);
-            if (lane == who) v = INFINITY;
-            if (lane == r) out = best;
-        }
-        if (lane < 8) part[((uint64_t)q * RT_CHUNKS + chunk) * 8 + lane] = out;
-    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int m = 0; m < 2; m++)
+            if (q0 + tq + k < nq && c0 + tc + m < ncent)
+                dist[(uint64_t)(q0 + tq + k) * ncent + c0 + tc + m] = acc[k][m];
 }
 
-// Step 2: one warp per query: the 8 smallest over the chunks, the features,
-// the network and the decision.
+// Step 2: one warp per query: the 8 smallest centroid distances, the
+// features, the network and the decision.
 __global__ void __launch_bounds__(256) router_route_kernel(
-    const float *__restrict__ queries, int dpad, const float *__restrict__ part,
-    const unsigned long long *__restrict__ popcnt, const int32_t *__restrict__ qprog,
+    const float *__restrict__ queries, int dpad, const float *__restrict__ dist,
+    int ncent, const unsigned long long *__restrict__ popcnt, const int32_t *__restrict__ qprog,
     uint64_t nrows, const uint32_t *__restrict__ kq, const int32_t *__restrict__ kind,
     const __nv_bfloat16 *__restrict__ w, const float *__restrict__ norm, float margin, int nq,
     float *__restrict__ feats, float *__restrict__ Z3, uint16_t *__restrict__ efq) {
@@ -945,18 +912,31 @@ __global__ void __launch_bounds__(256) router_route_kernel(
     const int q = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
     if (q >= nq) return;
     const float *qv = queries + (uint64_t)q * dpad;
+    // the 8 smallest of the query's centroid distances: each lane's sorted
+    // top-8 of its strided share, then 8 rounds of warp-wide minimum
     float mine = INFINITY;
     {
-        const float *pq = part + (uint64_t)q * RT_CHUNKS * 8;
-        float v0 = pq[lane], v1 = pq[32 + lane];  // RT_CHUNKS * 8 = 64 candidates
+        float top[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) top[i] = INFINITY;
+        const float *dq = dist + (uint64_t)q * ncent;
+        for (int c = lane; c < ncent; c += 32) {
+            float v = dq[c];
+            if (!(v < top[7])) continue;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const float t = top[i];
+                const bool sw = v < t;
+                top[i] = sw ? v : t;
+                v = sw ? t : v;
+            }
+        }
+        int head = 0;
         for (int r = 0; r < 8; r++) {
-            float best = fminf(v0, v1);
+            float best = head < 8 ? pick8(top, head) : INFINITY;
             int who = lane;
             warp_argmin(best, who);
-            if (lane == who) {  // remove one occurrence of the minimum
-                if (v0 <= v1) v0 = INFINITY;
-                else v1 = INFINITY;
-            }
+            if (lane == who) head++;
             if (lane == r) mine = best;
         }
     }
@@ -1108,7 +1088,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     const size_t fb = ((size_t)nq * NI * 4 + 255) & ~(size_t)255;
     const size_t zb = ((size_t)nq * NO * 4 + 255) & ~(size_t)255;
     const size_t eb = ((size_t)nq * 2 + 255) & ~(size_t)255;
-    const size_t pb8 = (size_t)nq * RT_CHUNKS * 8 * 4;  // centroid chunk minima
+    const size_t pb8 = plan ? 0 : (size_t)nq * r->ncent * 4;  // centroid distances
     const size_t gbytes = have_graph ? graph_out_layout(nq, FV_GPU_MAX_EF).bytes : 0;
     RT_OK(s.out_d.ensure(obytes));
     RT_OK(s.out_h.ensure(obytes));
@@ -1137,8 +1117,9 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     RT_OK(cudaStreamWaitEvent(side, ev[0], 0));
     g->launches += plan ? 1 : 2;
     if (!plan)
-        router_cent_kernel<<<dim3(RT_CHUNKS, nq), 128, 0, side>>>(
-            (const float *)(d + db.off_q), g->dpad, r->d_cent, r->ncent, dpart);
+        router_cent_kernel<<<dim3((r->ncent + RT_TC - 1) / RT_TC, (nq + RT_TQ - 1) / RT_TQ), 256, 0,
+                             side>>>((const float *)(d + db.off_q), nq, g->dpad, r->d_cent,
+                                     r->ncent, dpart);
     if (P > 0) {
         g->launches++;
         RT_OK(launch_bitmaps(g->d_cols, g->count, (const PredInsn *)(d + db.off_insns),
@@ -1151,7 +1132,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     RT_OK(cudaStreamWaitEvent(side, ev[1], 0));
     if (!plan) {
         router_route_kernel<<<(nq + 7) / 8, 256, 0, side>>>(
-            (const float *)(d + db.off_q), g->dpad, dpart,
+            (const float *)(d + db.off_q), g->dpad, dpart, r->ncent,
             s.popcnt.as<unsigned long long>(), (const int32_t *)(d + db.off_qprog), g->count,
             (const uint32_t *)dx, (const int32_t *)(dx + n4), r->mlp.w, r->mlp.norm, margin, nq,
             dfeat, dz, defq);
