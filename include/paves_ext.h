@@ -409,7 +409,7 @@ FvGpuIndex *pv_index_upload_prepared(const float *vectors, const double *cols,
                                      char *errbuf, size_t errlen);
 
 /* Shape of the tensor-core scan for later batches on g (0 = automatic):
- * epilogue warp groups (1, 2), pipeline stages (2..8), CTAs along rows per
+ * epilogue warp groups (1, 2, 3), pipeline stages (2..8), CTAs along rows per
  * query tile, query replicas down the tile (1, 2, 4; capped so that each
  * replica's share of a 128-row tile is at least 32 rows), seeding pass
  * (1 = always when the index has 8+ tiles per CTA, 2 = never; the main

@@ -192,7 +192,7 @@ extern "C" int pv_graph_stats(const FvGpuIndex *g, uint32_t *out, int nq) {
 extern "C" int pv_last_sparse(const FvGpuIndex *g) { return g ? g->last_sparse : 0; }
 
 extern "C" int pv_tc_shape(FvGpuIndex *g, int epi, int ns, int grow, int rep, int seed) {
-    if (!g || epi < 0 || epi > 2 || ns < 0 || ns > 8 || grow < 0 ||
+    if (!g || epi < 0 || epi > 3 || ns < 0 || ns > 8 || grow < 0 ||
         !(rep == 0 || rep == 1 || rep == 2 || rep == 4) || seed < 0 || seed > 2)
         return -1;
     std::lock_guard<std::mutex> lk(g->mu);

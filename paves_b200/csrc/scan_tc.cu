@@ -259,7 +259,7 @@ static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
 }
 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
-    if (!tc_supported(g) || (epi != 1 && epi != 2) || ns < 2 || ns > TC_MAX_STAGES) return false;
+    if (!tc_supported(g) || epi < 1 || epi > 3 || ns < 2 || ns > TC_MAX_STAGES) return false;
     const int S = tc_superset(g, topb, -1.f);
     if (!S) return false;
     const int KP = S < TC_MAX_LIST ? S : TC_MAX_LIST;
@@ -309,25 +309,34 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         snprintf(errbuf, errlen, "gpu: tensor-core scan not available for this batch");
         return -1;
     }
-    // two epilogue warp groups (each row half of a tile) when the lists fit,
-    // with at least two pipeline stages; else one group. The automatic shape
-    // stays within smem_pref, which leaves each SM a few KB for a small
-    // kernel beside the scan (the router's, a merge launched early).
+    // epilogue warp groups (each owning every EPI-th tile): two when the
+    // lists fit with at least two pipeline stages, else one (three groups
+    // measured no faster at batch 64: 0.0654 vs 0.0643 ms; pv_tc_shape can
+    // ask for them). The automatic shape stays within smem_pref, which
+    // leaves each SM a few KB for a small kernel beside the scan (the
+    // router's, a merge launched early).
     const size_t smem_cap = 227 * 1024;
     const size_t smem_pref = 222 * 1024;
     // stages: up to 128 KB of rows in flight
     const int ns0 = std::min(TC_MAX_STAGES, std::max(
         2, (int)(128 * 1024 / ((size_t)std::min(kblocks, TC_KBS) * TC_BOX))));
-    int EPI = 2, NS = ns0;
-    while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_pref) NS--;
-    if (tc_smem(kblocks, NS, KP, EPI) > smem_pref) {
+    int EPI = 0, NS = 0;
+    for (int e = 2; e >= 1 && !EPI; e--) {
+        const int nmin = e == 3 ? 3 : 2;
+        int n = ns0;
+        while (n > nmin && tc_smem(kblocks, n, KP, e) > smem_pref) n--;
+        if (n >= nmin && tc_smem(kblocks, n, KP, e) <= smem_pref) {
+            EPI = e;
+            NS = n;
+        }
+    }
+    if (!EPI) {  // the smallest shape, within the hard limit
         EPI = 1;
-        NS = ns0;
-        while (NS > 2 && tc_smem(kblocks, NS, KP, EPI) > smem_pref) NS--;
+        NS = 2;
     }
     if (g->tune_epi || g->tune_ns) {  // a tuned shape, if it fits
         const int e = g->tune_epi ? g->tune_epi : EPI, n = g->tune_ns ? g->tune_ns : NS;
-        if ((e == 1 || e == 2) && n >= 2 && n <= TC_MAX_STAGES &&
+        if (e >= 1 && e <= 3 && n >= 2 && n <= TC_MAX_STAGES &&
             tc_smem(kblocks, n, KP, e) <= smem_cap) {
             EPI = e;
             NS = n;
@@ -479,13 +488,16 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         }
     }
     // warm: a pass that starts without a bound (see tc_pass)
+    // (a warm pass with three groups would not fit its registers: it runs
+    // with two, inside the same shared-memory carve and dense runs)
     auto run = [&](const TcArgs &args, bool warm) {
         const int gr = args.grow * qtiles;
-        if (EPI == 2)
-            return warm ? tc_launch<2, true>(kind, gr, smem, g->stream, tmX, tmQ, args)
-                        : tc_launch<2, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
-        return warm ? tc_launch<1, true>(kind, gr, smem, g->stream, tmX, tmQ, args)
-                    : tc_launch<1, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
+        if (warm)
+            return EPI >= 2 ? tc_launch<2, true>(kind, gr, smem, g->stream, tmX, tmQ, args)
+                            : tc_launch<1, true>(kind, gr, smem, g->stream, tmX, tmQ, args);
+        if (EPI == 3) return tc_launch<3, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
+        if (EPI == 2) return tc_launch<2, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
+        return tc_launch<1, false>(kind, gr, smem, g->stream, tmX, tmQ, args);
     };
     FvHit *cand = (FvHit *)(c + off_cand);
     uint32_t *ccnt = (uint32_t *)(c + off_ccnt);

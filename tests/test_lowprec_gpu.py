@@ -142,7 +142,8 @@ def test_fp8_large_k_superset_certified_or_rerun(clustered):
 
 
 @pytest.mark.parametrize("epi,rep,nq", [(1, 4, 1), (1, 4, 24), (2, 2, 24), (1, 2, 64),
-                                        (2, 2, 64), (2, 1, 64), (1, 1, 40), (2, 4, 16)])
+                                        (2, 2, 64), (2, 1, 64), (1, 1, 40), (2, 4, 16),
+                                        (3, 2, 64), (3, 1, 100), (3, 4, 7)])
 def test_tc_epilogue_shapes_match_oracle(epi, rep, nq):
     """Every epilogue shape (warp groups x query replicas down the tile)
     returns exactly the oracle's top-k on integer rows: replicas split each
