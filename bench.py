@@ -308,6 +308,10 @@ KERNEL_CASES = {
     "bf16_b64_sel01": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 0),
     "bf16_b64_sel1": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 1),
     "fp8_b64": (64, _lib.FV_GPU_PREC_FP8, _lib.PV_MODE_LOW, None),
+    # one dense class per batch, as the headline's class batches (10 %, 95 %)
+    "bf16_b64_sel10": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 2),
+    "bf16_b64_sel95": (64, _lib.FV_GPU_PREC_BF16, _lib.PV_MODE_LOW, 5),
+    "exact_b64_sel10": (64, _lib.FV_GPU_PREC_FP32, _lib.PV_MODE_EXACT, 2),
     # graph: 200k x 128 rows, HNSW M=16 efC=100, 64 queries, 10% filter, ef 64
     "graph_b64": (64, None, None, None),
 }
@@ -347,7 +351,11 @@ def kernel_case(name, iters, tc_shape=None):
     b = prepared_batch(gi, ds.queries[:nq], bp, TOPK, mode)
     batch_run(b, 3)
     _, st = batch_run(b, iters, stages=True)
-    print(json.dumps({"case": name, "iters": iters,
+    # the stages are timed apart (an event between them stops the kernels of
+    # one stage from starting under the last kernel of the one before);
+    # total_ms is the same batch without them
+    tot, _ = batch_run(b, iters)
+    print(json.dumps({"case": name, "iters": iters, "total_ms": round(tot / iters, 4),
                       "stage_ms": [round(x / iters, 4) for x in st]}))
     _lib.lib().pv_batch_free(b)
     gi.close()

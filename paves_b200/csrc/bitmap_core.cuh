@@ -52,6 +52,7 @@ static __device__ __forceinline__ void bitmap_work(
     __shared__ double s_tlo[BM_PCH][PV_RANGE_MAX_TERMS], s_thi[BM_PCH][PV_RANGE_MAX_TERMS];
     __shared__ unsigned long long s_tbits[BM_PCH][PV_RANGE_MAX_TERMS];
     __shared__ int s_mcols;  // register columns that IN-set terms test
+    __shared__ int s_ucols;  // register columns that the chunk's programs read
     if (dcounts) {
         P = min(P, dcounts[0]);
         ninsns = min(ninsns, dcounts[1]);
@@ -94,7 +95,10 @@ static __device__ __forceinline__ void bitmap_work(
             s_prog[threadIdx.x] = pg;
             s_cnt[threadIdx.x] = 0;
         }
-        if (threadIdx.x == 0) s_mcols = 0;
+        if (threadIdx.x == 0) {
+            s_mcols = 0;
+            s_ucols = 0;
+        }
         __syncthreads();
         const PredInsn *ins = ins_sm ? s_ins : insns;
         if (threadIdx.x < BM_PCH) {
@@ -135,6 +139,21 @@ static __device__ __forceinline__ void bitmap_work(
                 }
             }
             s_nt[p] = nt;
+            // the register columns these programs read (a column past the
+            // register set reads the one that stands in for it below)
+            int used = 0;
+            if (p < np) {
+                if (nt >= 0) {
+                    for (int k = 0; k < nt; k++) used |= 1 << min(s_tcol[p][k] & 0xFFFF, 3);
+                } else {
+                    for (int i = 0; i < pg.ninsn; i++) {
+                        const PredInsn in = ins[pg.insn0 + i];
+                        if (in.kind == FV_NODE_CMP || in.kind == FV_NODE_IN)
+                            used |= 1 << ((unsigned)in.col < (unsigned)BM_REG_COLS ? in.col : 0);
+                    }
+                }
+            }
+            if (used) atomicOr(&s_ucols, used);
         }
         __syncthreads();
         const int mcols = s_mcols;
@@ -149,14 +168,15 @@ static __device__ __forceinline__ void bitmap_work(
                 live[j] = row[j] < nrows;
             }
             // with few columns, each row's values are read once into
-            // registers for all programs of the chunk
+            // registers for all programs of the chunk (only the columns they
+            // test: a one-column filter reads one column of the table)
             double cv[BM_REG_COLS][4];
             if (ncols <= BM_REG_COLS) {
 #pragma unroll
                 for (int cc = 0; cc < BM_REG_COLS; cc++)
 #pragma unroll
                     for (int j = 0; j < 4; j++)
-                        cv[cc][j] = (cc < ncols && live[j])
+                        cv[cc][j] = (cc < ncols && ((s_ucols >> cc) & 1) && live[j])
                                         ? __ldg(cols + (uint64_t)cc * nrows + row[j])
                                         : 0.0;
             }

@@ -156,10 +156,18 @@ dense_top32_kernel(const uint64_t *__restrict__ dense, uint64_t dcap, uint32_t *
                    uint8_t *__restrict__ trunc, unsigned long long *tau_out,
                    uint8_t *__restrict__ unc) {
     __shared__ uint64_t lists[DM_THREADS / 32][32];
+    // the batch's programs and the bitmap kernel's counts were written two
+    // or more kernels back (each kernel of the chain triggers the next only
+    // after its own wait): read them while the kernel ahead finishes
+    long long passing = -1;
+    if (threadIdx.x == 0) {
+        const int pg = qprog[blockIdx.x];
+        passing = (long long)(pg >= 0 ? popcnt[pg] : nrows);
+    }
     pdl_wait();
     pdl_trigger();
     dense_top32_query(blockIdx.x, lists, dense, dcap, dcnt, reset_cnt, fullmin, tau, KO, qprog,
-                      popcnt, nrows, out, out_cnt, trunc, tau_out, unc);
+                      popcnt, nrows, out, out_cnt, trunc, tau_out, unc, passing);
 }
 
 cudaError_t launch_dense_merge(const uint64_t *dense, uint64_t dcap, uint32_t *dcnt,

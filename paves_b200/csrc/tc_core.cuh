@@ -1007,8 +1007,8 @@ static __device__ __noinline__ void dense_merge_query(
 // folds in 32 new keys at a time (a shuffle bitonic sort of the new keys in
 // descending order, an elementwise min with the list, which leaves the 32
 // smallest as a bitonic sequence, and a bitonic clean back to ascending);
-// a batch none of whose keys beats the list's last key is skipped. Warp 0
-// then folds the other warps' lists into its own.
+// a batch none of whose keys beats the list's last key is skipped. The
+// warps' lists then fold pairwise into warp 0's.
 __device__ __forceinline__ uint64_t warp_sort32(uint64_t x, int lane, bool descending) {
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1)
@@ -1040,7 +1040,7 @@ __device__ __forceinline__ void dense_top32_query(
     const unsigned long long *tau, int KO, const int32_t *__restrict__ qprog,
     const unsigned long long *__restrict__ popcnt, uint64_t nrows, FvHit *__restrict__ out,
     uint32_t *__restrict__ out_cnt, uint8_t *__restrict__ trunc, unsigned long long *tau_out,
-    uint8_t *__restrict__ unc) {
+    uint8_t *__restrict__ unc, long long passing_pre = -1) {
     const int NW = blockDim.x >> 5;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned long long bound = tau ? tau[q] : KEY_MAX;
@@ -1066,15 +1066,21 @@ __device__ __forceinline__ void dense_top32_query(
             best = warp_clean32(best < d ? best : d, lane);
         }
     }
+    // the warps' lists fold pairwise, log2(NW) rounds (warp w takes in
+    // warp w + step's list, read descending, while w is a multiple of 2 step)
     lists[warp][lane] = best;
-    __syncthreads();
-    if (warp == 0) {
-        for (int w = 1; w < NW; w++) {
-            const uint64_t d = lists[w][31 - lane];  // descending
+    for (int step = 1; step < NW; step <<= 1) {
+        __syncthreads();
+        if ((warp & (2 * step - 1)) == 0 && warp + step < NW) {
+            const uint64_t d = lists[warp + step][31 - lane];
             const uint64_t m = best < d ? best : d;
-            if (!__any_sync(0xffffffffu, m != best)) continue;
-            best = warp_clean32(m, lane);
+            if (__any_sync(0xffffffffu, m != best)) {
+                best = warp_clean32(m, lane);
+                lists[warp][lane] = best;
+            }
         }
+    }
+    if (warp == 0) {
         const bool have = lane < KO && best != KEY_MAX;
         const int c = __popc(__ballot_sync(0xffffffffu, have));
         if (have) {
@@ -1086,8 +1092,11 @@ __device__ __forceinline__ void dense_top32_query(
         const uint64_t last = __shfl_sync(0xffffffffu, best, KO - 1);
         if (lane == 0) {
             out_cnt[q] = (uint32_t)c;
-            const int pg = qprog[q];
-            const unsigned long long passing = pg >= 0 ? popcnt[pg] : nrows;
+            unsigned long long passing = (unsigned long long)passing_pre;
+            if (passing_pre < 0) {
+                const int pg = qprog[q];
+                passing = pg >= 0 ? popcnt[pg] : nrows;
+            }
             trunc[q] = passing > (unsigned long long)KO ? 1 : 0;
             if (tau_out && c == KO && last < tau_out[q]) tau_out[q] = last;
             if (unc) {
