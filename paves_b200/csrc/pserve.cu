@@ -639,7 +639,9 @@ extern "C" PvServe *pv_serve_create(FvGpuIndex *g, int max_batch, uint32_t max_k
     a.bar_ns = s->bar_ns;
     a.timeout_ns = 2000000000ull;
     a.drain_ns = 2000000000ull;
-    a.merge_smem = s->smem - 1024 - (size_t)(2 * s->NS + 6 + 2 * TC_NR) * 8;
+    // (everything below the barriers: 2 per stage, per accumulator and per
+    // norm slot, plus the query-tile and drain barriers)
+    a.merge_smem = s->smem - 1024 - (size_t)(2 * s->NS + 2 * TC_NACC + 2 + 2 * TC_NR) * 8;
 
     // capture the launch once; replays restart the kernel
     {

@@ -53,7 +53,7 @@ scan_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled operand tiles
     unsigned char *base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    const TcSmem sm = tc_carve(base, a.kblocks, a.NS, a.KP, EPI);
+    const TcSmem sm = tc_carve(base, a.kblocks, a.NS, a.KP, EPI, KIND != TCK_TF32);
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     const int warp = threadIdx.x >> 5;
@@ -262,8 +262,8 @@ bool tc_supported(const FvGpuIndex *g) {
     return row_bytes <= 512;  // query tile <= 64 KB of shared memory
 }
 
-static size_t tc_smem(int kblocks, int NS, int KP, int EPI) {
-    return tc_smem_bytes(kblocks, NS, KP, EPI);
+static size_t tc_smem(int kblocks, int NS, int KP, int EPI, bool staged = true) {
+    return tc_smem_bytes(kblocks, NS, KP, EPI, staged);
 }
 
 bool tc_shape_fits(const FvGpuIndex *g, uint32_t topb, int epi, int ns) {
@@ -332,8 +332,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     for (int e = 2; e >= 1 && !EPI; e--) {
         const int nmin = e == 3 ? 3 : 2;
         int n = ns0;
-        while (n > nmin && tc_smem(kblocks, n, KP, e) > smem_pref) n--;
-        if (n >= nmin && tc_smem(kblocks, n, KP, e) <= smem_pref) {
+        while (n > nmin && tc_smem(kblocks, n, KP, e, !tf32) > smem_pref) n--;
+        if (n >= nmin && tc_smem(kblocks, n, KP, e, !tf32) <= smem_pref) {
             EPI = e;
             NS = n;
         }
@@ -345,12 +345,12 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
     if (g->tune_epi || g->tune_ns) {  // a tuned shape, if it fits
         const int e = g->tune_epi ? g->tune_epi : EPI, n = g->tune_ns ? g->tune_ns : NS;
         if (e >= 1 && e <= 3 && n >= 2 && n <= TC_MAX_STAGES &&
-            tc_smem(kblocks, n, KP, e) <= smem_cap) {
+            tc_smem(kblocks, n, KP, e, !tf32) <= smem_cap) {
             EPI = e;
             NS = n;
         }
     }
-    const size_t smem = tc_smem(kblocks, NS, KP, EPI);
+    const size_t smem = tc_smem(kblocks, NS, KP, EPI, !tf32);
     const int qtiles = (nq + TC_BM - 1) / TC_BM;
     const int nqpad = qtiles * TC_BM;
     // query replicas: as many as the batch leaves room for, while each

@@ -138,8 +138,10 @@ struct TcSmem {
     uint64_t *full, *empty, *tfull, *tempty, *qbar, *done, *nfull, *nempty;
 };
 
+// staged: the candidate staging slots exist (every kind but TF32, whose
+// admissions re-read the accumulator registers; its 32-32 KB go to stages)
 __device__ __forceinline__ TcSmem tc_carve(unsigned char *base, int KBt, int NS, int KPcap,
-                                           int EPI) {
+                                           int EPI, bool staged = true) {
     TcSmem m;
     m.sQ = base;                                       // KBt boxes
     m.sX = m.sQ + (size_t)KBt * TC_BOX;                // NS stages
@@ -150,7 +152,8 @@ __device__ __forceinline__ TcSmem tc_carve(unsigned char *base, int KBt, int NS,
     m.stage = (float *)(m.lists + (size_t)TC_BM * EPI * KPcap);
     // row norms (and fp8 scales, compacted-set row ids) of a tile, TC_NR
     // tiles in flight (slot = [norms 128][scales 128][row ids 128])
-    m.snorm = m.stage + 32 * TC_BM * EPI;
+    m.snorm = m.stage + (staged ? 32 * TC_BM * EPI : 0);
+    if (!staged) m.stage = nullptr;
     uint64_t *bars = (uint64_t *)(m.snorm + (size_t)TC_NR * TC_NSLOT_F);
     m.full = bars;              // [NS]
     m.empty = m.full + NS;      // [NS]
@@ -163,10 +166,10 @@ __device__ __forceinline__ TcSmem tc_carve(unsigned char *base, int KBt, int NS,
     return m;
 }
 
-inline size_t tc_smem_bytes(int kblocks, int NS, int KPcap, int EPI) {
+inline size_t tc_smem_bytes(int kblocks, int NS, int KPcap, int EPI, bool staged = true) {
     return 1024 + (size_t)kblocks * TC_BOX +
            (size_t)NS * (kblocks < TC_KBS ? kblocks : TC_KBS) * TC_BOX +
-           (size_t)TC_BM * EPI * KPcap * 8 + (size_t)32 * TC_BM * EPI * 4 +
+           (size_t)TC_BM * EPI * KPcap * 8 + (staged ? (size_t)32 * TC_BM * EPI * 4 : 0) +
            (size_t)TC_NR * TC_NSLOT_F * 4 + (size_t)(2 * NS + 2 * TC_NACC + 2 + 2 * TC_NR) * 8;
 }
 
@@ -477,7 +480,21 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
             auto chunk = [&](const int c, const uint32_t(&r)[32]) {
                 // hot loop: distances and a candidate mask only; the rare
                 // admissions run below, outside the unrolled code (a negative
-                // norm-form value is clamped there)
+                // norm-form value is clamped there). They take a candidate's
+                // distance from the staging slots, or, in a TF32 pass, again
+                // from the accumulator registers (the same operations on the
+                // same values: the same bits), whose freed shared memory
+                // holds a third stage of its 512-byte rows: measured at batch
+                // 64 the TF32 pass ran 0.098 vs 0.102 ms; the BF16 pass the
+                // same way ran 0.069 vs 0.064 ms (its accumulators stay live
+                // through the admissions: 144 registers instead of 128, and
+                // more stages did not help it)
+                constexpr bool RECOMP = KIND == TCK_TF32;
+                auto dist_of = [&](const int i, const uint32_t acc_bits) -> float {
+                    float dot = __uint_as_float(acc_bits);
+                    if (FP8) dot *= xsv[c * 32 + i] * qs;
+                    return fmaf(-2.f, dot, xnv[c * 32 + i] + qn);
+                };
                 uint32_t cmask = 0;
 #pragma unroll
                 for (int i4 = 0; i4 < 32; i4 += 4) {
@@ -493,7 +510,7 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                         if (FP8) dot *= xsa[u] * qs;
                         const float d = fmaf(-2.f, dot, xna[u] + qn);
                         if (d <= thr_d) {
-                            stage[i * NSLOT + slot] = d;
+                            if (!RECOMP) stage[i * NSLOT + slot] = d;
                             cmask |= 1u << i;
                         }
                     }
@@ -509,8 +526,9 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                     float v[32];
 #pragma unroll
                     for (int i = 0; i < 32; i++)
-                        v[i] = ((cmask >> i) & 1u) ? fmaxf(stage[i * NSLOT + slot], 0.f)
-                                                   : __int_as_float(0x7f800000);
+                        v[i] = ((cmask >> i) & 1u)
+                                   ? fmaxf(RECOMP ? dist_of(i, r[i]) : stage[i * NSLOT + slot], 0.f)
+                                   : __int_as_float(0x7f800000);
                     float kth = -1.f;
                     for (int cnt = 0; cnt < KP;) {
                         float m = __int_as_float(0x7f800000);
@@ -532,7 +550,17 @@ __device__ __forceinline__ bool tc_pass(const CUtensorMap *tmXp, const CUtensorM
                 while (cmask) {
                     const int i = __ffs(cmask) - 1;
                     cmask &= cmask - 1;
-                    const float d = fmaxf(stage[i * NSLOT + slot], 0.f);
+                    float dv;
+                    if (RECOMP) {
+                        uint32_t bits = 0;
+#pragma unroll
+                        for (int j = 0; j < 32; j++)
+                            if (j == i) bits = r[j];
+                        dv = dist_of(i, bits);
+                    } else {
+                        dv = stage[i * NSLOT + slot];
+                    }
+                    const float d = fmaxf(dv, 0.f);
                     const uint64_t row = rbase + c * 32 + i;
                     const uint32_t rid = a.rowids ? ridv[c * 32 + i] : (uint32_t)row;
                     const uint64_t key = make_key(d, rid);
