@@ -57,6 +57,25 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
     if (!pb.insns.empty())
         memcpy(h + db.off_insns, pb.insns.data(), pb.insns.size() * sizeof(PredInsn));
     if (!pb.consts.empty()) memcpy(h + db.off_consts, pb.consts.data(), pb.consts.size() * 8);
+    // one range-form program with well-formed terms: the lean bitmap kernel
+    db.one_range = false;
+    if (P == 1 && pb.progs[0].ninsn == 1 && pb.progs[0].insn0 >= 0 &&
+        pb.progs[0].insn0 < (int)pb.insns.size() &&
+        pb.insns[pb.progs[0].insn0].kind == PV_NODE_RANGE) {
+        const PredInsn &r = pb.insns[pb.progs[0].insn0];
+        bool ok = r.n >= 1 && r.n <= PV_RANGE_MAX_TERMS;
+        int ci = r.val0;
+        const int nc = (int)pb.consts.size();
+        for (int k = 0; k < r.n && ok; k++) {
+            ok = ci >= 0 && ci + 2 <= nc;
+            if (!ok) break;
+            const int meta = (int)pb.consts[ci];
+            const bool mask = meta & PV_TERM_MASK;
+            ok = (meta & 0xFFFF) < g->ncols && (mask || ci + 3 <= nc);
+            ci += mask ? 2 : 3;
+        }
+        db.one_range = ok;
+    }
     // sparse route: one filter shared by the whole batch whose matches are
     // bounded by a small count (the scan then reads only those rows)
     db.sparse_bound = 0;
@@ -115,7 +134,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         PV_CUDA_OK(launch_bitmaps(g->d_cols, g->count, d_insns, d_progs, d_consts, P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
                                   s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                                  db.ninsns, db.nconsts, g->ncols),
+                                  db.ninsns, db.nconsts, g->ncols, db.one_range),
                    errbuf, errlen);
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);

@@ -675,7 +675,7 @@ int graph_run_host(FvGpuIndex *g, int nq, const float *queries, const uint32_t *
                                   (const double *)(d + db.off_consts), P,
                                   s.bitmaps.as<uint32_t>(), bm_words,
                                   s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                                  db.ninsns, db.nconsts, g->ncols),
+                                  db.ninsns, db.nconsts, g->ncols, db.one_range),
                    errbuf, errlen);
     }
     const GraphOut lo = graph_out_layout(nq, ef);

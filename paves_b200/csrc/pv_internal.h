@@ -21,7 +21,7 @@ cudaError_t launch_bitmaps(const double *cols, uint64_t nrows, const PredInsn *i
                            const PredProg *progs, const double *consts, int P,
                            uint32_t *bitmaps, uint64_t bm_words, unsigned long long *popcnt,
                            int sm_count, cudaStream_t st, int ninsns, int nconsts,
-                           int ncols = 1 << 30);
+                           int ncols = 1 << 30, bool one_range = false);
 // Same, with the batch's {P, ninsns, nconsts} read on the device from
 // dcounts (each at most its cap): one launch shape for a CUDA graph.
 cudaError_t launch_bitmaps_capped(const double *cols, uint64_t nrows, const PredInsn *insns,
@@ -102,6 +102,9 @@ struct DevBatch {
     // sparse route: every query uses program 0, whose matches are at most
     // sparse_bound rows (0 = dense)
     uint64_t sparse_bound = 0;
+    // one program in range form whose terms are all well formed (constants
+    // in the pool, columns in the table): the lean bitmap kernel
+    bool one_range = false;
 };
 
 int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,

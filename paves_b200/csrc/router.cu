@@ -600,7 +600,7 @@ extern "C" int pv_router_features(PvRouter *r, FvGpuIndex *g, int nq, const floa
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
                              bm_words, s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                             db.ninsns, db.nconsts, g->ncols));
+                             db.ninsns, db.nconsts, g->ncols, db.one_range));
     }
     const size_t fbytes = (size_t)nq * NI * 4;
     RT_OK(s.out_d.ensure(fbytes));
@@ -1126,7 +1126,7 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                              (const PredProg *)(d + db.off_progs),
                              (const double *)(d + db.off_consts), P, s.bitmaps.as<uint32_t>(),
                              bm_words, s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
-                             db.ninsns, db.nconsts, g->ncols));
+                             db.ninsns, db.nconsts, g->ncols, db.one_range));
     }
     RT_OK(cudaEventRecord(ev[1], g->stream));
     RT_OK(cudaStreamWaitEvent(side, ev[1], 0));
