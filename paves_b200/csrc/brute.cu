@@ -139,6 +139,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
+    // this batch just launched its bitmap kernel (query prep may run beside it)
+    const bool bm_launched = !bitmaps_ready && !db.counts_on_device && P > 0;
     g->last_sparse = 0;
     g->last_exact_tc = 0;
     if (db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024) {
@@ -174,7 +176,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
                   db.nconsts};
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
-                           errbuf, errlen, db.counts_on_device ? &lz : nullptr))
+                           errbuf, errlen, db.counts_on_device ? &lz : nullptr, false, nullptr,
+                           bm_launched))
             return -1;
         if (ev) cudaEventRecord(ev[4], g->stream);
         return 0;
@@ -185,7 +188,8 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
                   db.nconsts};
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
-                           errbuf, errlen, db.counts_on_device ? &lz : nullptr, true))
+                           errbuf, errlen, db.counts_on_device ? &lz : nullptr, true, nullptr,
+                           bm_launched))
             return -1;
         g->last_exact_tc = 1;
         if (ev) cudaEventRecord(ev[4], g->stream);

@@ -197,7 +197,9 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
                    size_t errlen, const TcLazy *lz = nullptr, bool tf32 = false,
-                   const TcRowSet *rs = nullptr);
+                   const TcRowSet *rs = nullptr, bool behind_bitmaps = false);
+// behind_bitmaps: the last launch on the stream is this batch's bitmap
+// kernel (query prep then runs beside it)
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);

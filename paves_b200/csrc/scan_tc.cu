@@ -93,13 +93,23 @@ __global__ void query_prep_kernel(const float *__restrict__ q, int nq, int dpad,
                                   unsigned char *__restrict__ out, float *__restrict__ qnorm,
                                   float *__restrict__ qscale, unsigned long long *__restrict__ tau,
                                   uint32_t *__restrict__ dcnt,
-                                  unsigned long long *__restrict__ fullmin, int *__restrict__ err) {
-    pdl_wait();
-    pdl_trigger();
+                                  unsigned long long *__restrict__ fullmin, int *__restrict__ err,
+                                  int behind_bitmaps) {
+    // behind_bitmaps: the kernel ahead is this batch's bitmap kernel, which
+    // touches nothing this one reads or writes (the queries were copied
+    // before it), so the work runs beside it and only the completion waits
+    if (!behind_bitmaps) {
+        pdl_wait();
+        pdl_trigger();
+    }
     const int qi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (qi >= nqpad) return;
-    query_prep_row(qi, threadIdx.x & 31, q, nq, dpad, dim, bq, kelems, kind, out, qnorm, qscale,
-                   tau, dcnt, fullmin, err);
+    if (qi < nqpad)
+        query_prep_row(qi, threadIdx.x & 31, q, nq, dpad, dim, bq, kelems, kind, out, qnorm,
+                       qscale, tau, dcnt, fullmin, err);
+    if (behind_bitmaps) {
+        pdl_wait();
+        pdl_trigger();
+    }
 }
 
 // ---------------------------------------------------------------- re-rank
@@ -301,7 +311,8 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const uint32_t *bitmaps, uint64_t bm_words,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
-                   size_t errlen, const TcLazy *lz, bool tf32, const TcRowSet *rs) {
+                   size_t errlen, const TcLazy *lz, bool tf32, const TcRowSet *rs,
+                   bool behind_bitmaps) {
     const bool fp8 = !tf32 && g->precision == FV_GPU_PREC_FP8;
     const int kind = tf32 ? TCK_TF32 : fp8 ? TCK_FP8 : TCK_BF16;
     const int esz = tck_esz(kind);
@@ -401,7 +412,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                           nq, g->dpad, g->dim, nqpad, R > 1 ? bq : nqpad, kelems, kind, c,
                           (float *)(c + off_qn), fp8 ? (float *)(c + off_qs) : nullptr,
                           s.tau.as<unsigned long long>(), d_dcnt,
-                          certify ? d_fullmin : nullptr, d_err),
+                          certify ? d_fullmin : nullptr, d_err, behind_bitmaps ? 1 : 0),
                errbuf, errlen);
 
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
