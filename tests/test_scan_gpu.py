@@ -264,4 +264,12 @@ def test_range_form_edge_values():
     check_exact(ids, dists, cnt, trunc, o[0], o[2], o[3], o[4], 4096)
     for i, p in enumerate(preds):
         assert _bound(g, p) >= int(o[4][i]), p
+    # each predicate alone: a batch sharing one range-form filter takes the
+    # lean bitmap kernel, the others the general one; both as the oracle
+    for i, p in enumerate(preds):
+        q2 = np.repeat(ds.queries[:1], 2, axis=0)
+        ids2, dists2, cnt2, trunc2 = g.brute_batch(q2, [p, p], 4096)
+        for j in range(2):
+            check_exact(ids2[j:j + 1], dists2[j:j + 1], cnt2[j:j + 1], trunc2[j:j + 1],
+                        o[0][i:i + 1], o[2][i:i + 1], o[3][i:i + 1], o[4][i:i + 1], 4096)
     g.close()
