@@ -103,7 +103,7 @@ int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen) {
 // Device-side work of one batch: inputs already resident in db.stage_d.
 int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
                  uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
-                 cudaEvent_t *ev, bool bitmaps_ready) {
+                 cudaEvent_t *ev, bool bitmaps_ready, cudaEvent_t bm_done) {
     const int nq = db.nq, P = db.P;
     char *d = db.stage_d->as<char>();
     const float *d_q = (const float *)(d + db.off_q);
@@ -139,11 +139,24 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
     } else {
         PV_CUDA_OK(s.popcnt.ensure(8), errbuf, errlen);
     }
-    // this batch just launched its bitmap kernel (query prep may run beside it)
-    const bool bm_launched = !bitmaps_ready && !db.counts_on_device && P > 0;
+    // this batch's bitmap kernel is the last launch on the stream (query
+    // prep may run beside it): launched here, or by a caller that says so
+    // by asking for bm_done
+    const bool bm_launched =
+        !db.counts_on_device && P > 0 && (!bitmaps_ready || bm_done != nullptr);
+    const bool sparse_route = db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024;
+    const bool low_tc_route =
+        !sparse_route && mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0;
+    const bool exact_tc_route = !sparse_route && !low_tc_route && mode == PV_MODE_EXACT &&
+                                nq >= PV_EXACT_TC_MIN_NQ && tf32_supported(g) &&
+                                tf32_superset(g, topb, db.q_amax) > 0;
+    // bm_done: the bitmaps are complete once query prep, run beside them,
+    // completes (tensor-core routes), else at once in stream order
+    if (bm_done && !(low_tc_route || exact_tc_route))
+        PV_CUDA_OK(cudaEventRecord(bm_done, g->stream), errbuf, errlen);
     g->last_sparse = 0;
     g->last_exact_tc = 0;
-    if (db.sparse_bound > 0 && !db.counts_on_device && topb <= 1024) {
+    if (sparse_route) {
         g->last_sparse = 1;
         // the matching rows on the tensor cores, when the mode scans there
         const bool low_tc = mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0;
@@ -169,7 +182,7 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         }
         return 0;
     }
-    if (mode == 1 && tc_supported(g) && tc_superset(g, topb, db.q_amax) > 0) {
+    if (low_tc_route) {
         // a staged batch with its counts on the device (the stream's graphs)
         // may mark itself lazy: then it has no bitmaps (see stream.cu)
         TcLazy lz{(const int *)(d + db.off_counts) + 3, d_progs, d_insns, d_consts,
@@ -177,19 +190,18 @@ int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
                            errbuf, errlen, db.counts_on_device ? &lz : nullptr, false, nullptr,
-                           bm_launched))
+                           bm_launched, bm_done))
             return -1;
         if (ev) cudaEventRecord(ev[4], g->stream);
         return 0;
     }
-    if (mode == PV_MODE_EXACT && nq >= PV_EXACT_TC_MIN_NQ && tf32_supported(g) &&
-        tf32_superset(g, topb, db.q_amax) > 0) {
+    if (exact_tc_route) {
         TcLazy lz{(const int *)(d + db.off_counts) + 3, d_progs, d_insns, d_consts,
                   db.nconsts};
         if (launch_scan_tc(g, nq, db.q_amax, d_q, d_qprog, s.bitmaps.as<uint32_t>(), bm_words,
                            s.popcnt.as<unsigned long long>(), topb, d_out, d_cnt, d_trunc, ev,
                            errbuf, errlen, db.counts_on_device ? &lz : nullptr, true, nullptr,
-                           bm_launched))
+                           bm_launched, bm_done))
             return -1;
         g->last_exact_tc = 1;
         if (ev) cudaEventRecord(ev[4], g->stream);

@@ -111,11 +111,15 @@ int brute_prepare(FvGpuIndex *g, int nq, const float *queries, const PredBatch &
                   DevBatch &db, size_t extra_bytes, char *errbuf, size_t errlen);
 int brute_upload(FvGpuIndex *g, DevBatch &db, char *errbuf, size_t errlen);
 // ev (optional): 5 events recorded before bitmaps, before scan, after scan,
-// after re-rank and after merge. bitmaps_ready: the batch's bitmaps and
+// after re-rank and after merge. bm_done (with bitmaps_ready: the caller's
+// bitmap kernel is the last launch on the stream): recorded once the
+// bitmaps are complete (behind query prep, which runs beside them, on the
+// tensor-core routes). bitmaps_ready: the batch's bitmaps and
 // popcounts are already in g->scan (no bitmap launch).
 int brute_launch(FvGpuIndex *g, DevBatch &db, uint32_t topb, int mode, FvHit *d_out,
                  uint32_t *d_cnt, uint8_t *d_trunc, char *errbuf, size_t errlen,
-                 cudaEvent_t *ev = nullptr, bool bitmaps_ready = false);
+                 cudaEvent_t *ev = nullptr, bool bitmaps_ready = false,
+                 cudaEvent_t bm_done = nullptr);
 // Re-runs exactly the queries with unc[q] != 0 on g (host buffers; call with
 // g->mu held) and writes their results over out / out_cnt / truncated.
 int redo_flagged(FvGpuIndex *g, int nq, const float *queries, const PredBatch &pb,
@@ -197,9 +201,11 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
                    size_t errlen, const TcLazy *lz = nullptr, bool tf32 = false,
-                   const TcRowSet *rs = nullptr, bool behind_bitmaps = false);
+                   const TcRowSet *rs = nullptr, bool behind_bitmaps = false,
+                   cudaEvent_t prep_done = nullptr);
 // behind_bitmaps: the last launch on the stream is this batch's bitmap
-// kernel (query prep then runs beside it)
+// kernel (query prep then runs beside it); prep_done: recorded behind
+// query prep
 // Reads and clears the watchdog word of the last tensor-core scan after the
 // stream was synchronized; -1 + errbuf if a bounded wait expired.
 int check_tc_watchdog(FvGpuIndex *g, char *errbuf, size_t errlen);

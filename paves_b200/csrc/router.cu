@@ -1128,7 +1128,28 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
                              bm_words, s.popcnt.as<unsigned long long>(), g->sm_count, g->stream,
                              db.ninsns, db.nconsts, g->ncols, db.one_range));
     }
-    RT_OK(cudaEventRecord(ev[1], g->stream));
+    // Speculative scan on the main stream meanwhile: a scan costs about the
+    // same for one query as for the batch and is exact, so it runs unless
+    // a caller's plan sends every query to the graph; the router's answer
+    // only decides whether its results are replaced by the graph search's.
+    bool plan_all_graph = plan != nullptr && have_graph;
+    for (int i = 0; plan_all_graph && i < nq; i++) plan_all_graph = plan[i] > 0;
+    const bool spec = !plan_all_graph;
+    if (spec) {
+        char *od = s.out_d.as<char>();
+        const int mode = g->precision != FV_GPU_PREC_FP32 ? PV_MODE_LOW : PV_MODE_EXACT;
+        // ev[1]: the bitmaps are complete (behind query prep, which the
+        // tensor-core scan runs beside them); the routing waits for it
+        if (brute_launch(g, db, topb, mode, (FvHit *)od, (uint32_t *)(od + off_cnt),
+                         (uint8_t *)(od + off_tr), errbuf, errlen, nullptr, true, ev[1]))
+            return -1;
+        RT_OK(cudaEventRecord(ev[3], g->stream));
+        RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
+        // the watchdog word rides behind the results (the spare tail of out_h)
+        tc_watchdog_enqueue(g, (int *)(s.out_h.as<char>() + obytes - 64));
+    } else {
+        RT_OK(cudaEventRecord(ev[1], g->stream));
+    }
     RT_OK(cudaStreamWaitEvent(side, ev[1], 0));
     if (!plan) {
         router_route_kernel<<<(nq + 7) / 8, 256, 0, side>>>(
@@ -1144,24 +1165,6 @@ extern "C" int pv_routed_batch(FvGpuIndex *g, PvRouter *r, int nq, const float *
     RT_OK(cudaEventRecord(ev[5], side));
     RT_OK(cudaMemcpyAsync(hefq, defq, (size_t)nq * 2, cudaMemcpyDeviceToHost, side));
     RT_OK(cudaEventRecord(ev[2], side));
-    // Speculative scan on the main stream meanwhile: a scan costs about the
-    // same for one query as for the batch and is exact, so it runs unless
-    // a caller's plan sends every query to the graph; the router's answer
-    // only decides whether its results are replaced by the graph search's.
-    bool plan_all_graph = plan != nullptr && have_graph;
-    for (int i = 0; plan_all_graph && i < nq; i++) plan_all_graph = plan[i] > 0;
-    const bool spec = !plan_all_graph;
-    if (spec) {
-        char *od = s.out_d.as<char>();
-        const int mode = g->precision != FV_GPU_PREC_FP32 ? PV_MODE_LOW : PV_MODE_EXACT;
-        if (brute_launch(g, db, topb, mode, (FvHit *)od, (uint32_t *)(od + off_cnt),
-                         (uint8_t *)(od + off_tr), errbuf, errlen, nullptr, true))
-            return -1;
-        RT_OK(cudaEventRecord(ev[3], g->stream));
-        RT_OK(cudaMemcpyAsync(s.out_h.p, od, obytes, cudaMemcpyDeviceToHost, g->stream));
-        // the watchdog word rides behind the results (the spare tail of out_h)
-        tc_watchdog_enqueue(g, (int *)(s.out_h.as<char>() + obytes - 64));
-    }
     RT_OK(cudaEventSynchronize(ev[2]));
     // each query takes the route the router chose for it: the graph search
     // at its beam width (graph-routed queries, when the index has a graph)

@@ -312,7 +312,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                    const unsigned long long *popcnt, uint32_t topb, FvHit *d_out,
                    uint32_t *d_cnt, uint8_t *d_trunc, cudaEvent_t *ev, char *errbuf,
                    size_t errlen, const TcLazy *lz, bool tf32, const TcRowSet *rs,
-                   bool behind_bitmaps) {
+                   bool behind_bitmaps, cudaEvent_t prep_done) {
     const bool fp8 = !tf32 && g->precision == FV_GPU_PREC_FP8;
     const int kind = tf32 ? TCK_TF32 : fp8 ? TCK_FP8 : TCK_BF16;
     const int esz = tck_esz(kind);
@@ -414,6 +414,7 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
                           s.tau.as<unsigned long long>(), d_dcnt,
                           certify ? d_fullmin : nullptr, d_err, behind_bitmaps ? 1 : 0),
                errbuf, errlen);
+    if (prep_done) PV_CUDA_OK(cudaEventRecord(prep_done, g->stream), errbuf, errlen);
 
     static_assert(sizeof(CUtensorMap) == sizeof(g->tmap_x), "CUtensorMap size");
     CUtensorMap tmX, tmQ;
