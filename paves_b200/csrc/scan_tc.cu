@@ -540,10 +540,13 @@ int launch_scan_tc(FvGpuIndex *g, int nq, float q_amax, const float *d_q,
         // sample still bounds the S-th key of the scan, and a short run
         // keeps the merge cheap (the radix select of S > 32 reads its run
         // 8 times). The sample's S best keys are spread over many lists
-        // (S / nlists per list on average), so a list rarely holds more
-        // than two of them: 4S keys in all, at least two per list, never
-        // more than the main pass's list length (its shared memory).
-        sa.kwrite = std::min(KP, std::max(2, (4 * S + nlists - 1) / std::max(1, nlists)));
+        // (S / nlists per list on average): 4S keys in all, at least one
+        // per list, never more than the main pass's list length (its
+        // shared memory). One key per list when that suffices measured
+        // 3.5 µs less before the main pass than two (batch 64, S = 10,
+        // 592 lists: heaps of one, half the seeding merge's keys), for a
+        // bound barely looser (the main pass ran the same).
+        sa.kwrite = std::min(KP, std::max(1, (4 * S + nlists - 1) / std::max(1, nlists)));
         // lists need hold no more than that (short heaps admit fewer rows);
         // a full list's last key bounds the S-th key only if it holds S
         sa.KP = sa.kwrite;
